@@ -1,0 +1,292 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 FTLM engine: H*v HBM GB/s on the 4x4 U=7 production block.
+
+Workload (one step): the largest momentum block of the batched 4x4 production
+curve (lx=ly=4, tx=ty=1, t'=0, U=7, V=0; sector N_up=N_down=8, k=(0,0),
+dim ~1.04e7): FTLM with 128 random vectors x 80 Lanczos steps run as one
+multi-vector sweep per step, mixed precision (FP32 complex vectors and H*V,
+FP64 dot products / norms / alpha-beta / tridiagonal), Philox uniform-phase
+start vectors; the Ritz values and weights of all 128 samples are produced on
+the device. With --gpus N each rank runs its own k-block of the same sector
+(weak scaling); there is no data-path collective.
+
+Metric: H*v HBM GB/s = algorithmic H*V bytes / time, with bytes per H*V
+launch D*[nvec*s*(1+h_nz) + nvec*s + m] (s = 8 B per FP32 complex, h_nz =
+nonzero-amplitude hops per row, m = 8 B per row). `value` divides by the
+whole step (Lanczos updates, reductions, tridiagonal solve included);
+`roofline.achieved` divides by the H*V kernel's own CUDA-event time.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "H*v HBM GB/s; sec per n(mu) curve, mixed vs FP64 GPU at |dn|<=1e-4"
+MODEL = dict(lx=4, ly=4, tx=1.0, ty=1.0, tp=0.0, phix=1.0, phiy=1.0, u=7.0, v=0.0)
+SECTOR = (8, 8)
+SAMPLES, STEPS = 128, 80
+FALLBACK_HBM = 6650.0
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def hbm_peak():
+    p = os.path.join(HERE, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def ncu_traffic():
+    """DRAM bytes per H*V launch from the committed ncu summary, if any."""
+    p = os.path.join(HERE, "profiles", "hv_block88_traffic.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["dram_bytes_per_launch"])
+    except Exception:
+        return None
+
+
+def cpu_baseline(threads: int):
+    """The reference's own apply_hamiltonian (oracle/_ref/ref_bench, compiled
+    from the reference sources) on a bounded sample: same lattice and
+    couplings, the largest sector it builds in seconds, 16 vectors x 2 sweeps."""
+    exe = os.path.join(HERE, "oracle", "_ref", "ref_bench")
+    if not os.path.exists(exe):
+        return None
+    args = [exe, "hv", "4", "4", "0", "0", "16", "2", "--", "--lx", "4", "--ly", "4", "--u", "7",
+            "--threads", str(threads), "--max-sector-dim", "100000000"]
+    r = subprocess.run(args, capture_output=True, text=True, env={**os.environ, "OPENBLAS_NUM_THREADS": "1"})
+    if r.returncode != 0:
+        return None
+    j = json.loads(r.stdout.strip().splitlines()[-1])
+    D, nz, nv, sw = j["dim"], j["nnz_nonzero"], j["nvec"], j["sweeps"]
+    bytes_per_sweep = D * nv * 16 * 2 + nz * nv * 16 + D * 8
+    gbs = bytes_per_sweep * sw / j["seconds"] / 1e9
+    return {"value": gbs, "unit": "GB/s", "cores": j["threads"], "kind": "reference",
+            "sample": (f"reference apply_hamiltonian (FP64 CSR SpMV, OpenMP over vectors) on 4x4 U=7 "
+                       f"sector (4,4) k=(0,0), dim {D}, {nv} vectors x {sw} sweeps, "
+                       f"{j['seconds']:.3f} s; sector (8,8) itself needs ~15 min/30 GB to build on the CPU")}
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    base = cpu_baseline(threads)
+    if base is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_bench not built (make -C oracle ref)"}))
+        return
+    vals = []
+    for _ in range(args.warmup + args.steps):
+        b = cpu_baseline(threads)
+        vals.append(b["value"])
+    v = statistics.median(vals[args.warmup:]) if len(vals) > args.warmup else base["value"]
+    line = {"metric": METRIC, "value": v, "unit": "GB/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "c128", "data": "synthetic (model-defined Hilbert space, Gaussian vectors)",
+            "impl": "reference",
+            "config": {"workload": "4x4 U=7 t'=0 FTLM H*V, sector (8,8) k=(0,0), 128 vectors x 80 steps"},
+            "cpu_baseline": {**base, "value": v},
+            "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    import ftlm_extended_hubbard_development_b200 as pkg
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl" if torch.cuda.is_available() else "gloo",
+                                timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    model = pkg.Model(**MODEL)
+    prec = pkg.engine.PREC_MIXED if args.precision == "mixed" else pkg.engine.PREC_FP64
+    opts = pkg.RunOpts(samples=SAMPLES, lanczos_steps=STEPS, exact_block_threshold=256,
+                       precision=prec, start_vector=pkg.engine.START_PHILOX_PHASE,
+                       batch_vectors=args.batch, device=local)
+    eng = pkg.Engine(model, opts)
+    info = eng.sector_prepare(*SECTOR)
+    k = rank % len(info.block_dims)
+    mx, my = k % model.lx, k // model.lx
+    dim = info.block_dims[k]
+
+    def barrier():
+        if ws > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        eng.spectra_reset()
+        eng.block_spectrum(mx, my, fetch=False)
+    eng.profile(True)
+    eng.profile_reset()
+    barrier()
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            eng.spectra_reset()
+            eng.block_spectrum(mx, my, fetch=False)
+        barrier()
+    prof = eng.profile()
+    dev_s = prof["block_ms"] / 1e3
+    t = torch.tensor([dev_s], dtype=torch.float64, device="cuda")
+    b = torch.tensor([prof["hv_bytes"]], dtype=torch.float64, device="cuda")
+    if ws > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        torch.distributed.all_reduce(b, op=torch.distributed.ReduceOp.SUM)
+    dev_s_max, bytes_all = float(t.item()), float(b.item())
+    value = bytes_all / dev_s_max / 1e9
+    achieved = prof["hv_bytes"] / (prof["hv_ms"] / 1e3) / 1e9
+    peak, peak_kind = hbm_peak()
+    bytes_per_launch = prof["hv_bytes"] / max(prof["hv_launches"], 1)
+
+    # e2e through the C ABI: tables from the model, spectrum and thermodynamic
+    # sums read back to host buffers every step
+    mu = pkg.linspace(-3.0, 4.0, 281)
+    betas = np.array([2.857142857142857, 12.5])
+    eng.profile_reset()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        eng.thermo_configure(betas, mu)
+        eng.sector_prepare(*SECTOR)
+        ev, w, pref = eng.block_spectrum(mx, my)
+        eng.thermo_accumulate_block(mx, my)
+        eng.thermo_read()
+    barrier()
+    e2e_s = time.perf_counter() - t0
+    pe = eng.profile()
+    e2e_t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if ws > 1:
+        torch.distributed.all_reduce(e2e_t, op=torch.distributed.ReduceOp.MAX)
+    e2e_val = bytes_all / float(e2e_t.item()) / 1e9
+
+    if rank == 0:
+        base = cpu_baseline(os.cpu_count() or 1) if (ws == 1 and not args.no_cpu_baseline) else None
+        line = {
+            "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dev_s_max * 1e3 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "c64 vectors, f64 reductions" if prec == pkg.engine.PREC_MIXED else "c128",
+            "data": "synthetic (model-defined Hilbert space; Philox uniform-phase start vectors)",
+            "config": {"workload": (f"4x4 U=7 t'=0 FTLM block, sector (8,8) k=({mx},{my}) dim {dim}: "
+                                    f"{SAMPLES} vectors x {STEPS} Lanczos steps per step, "
+                                    f"{args.precision}"),
+                       "lattice": "4x4", "sector": list(SECTOR), "k": [mx, my], "dim": dim,
+                       "samples": SAMPLES, "lanczos_steps": STEPS, "precision": args.precision,
+                       "batch_vectors": args.batch or min(SAMPLES, 128),
+                       "l2": "inputs larger than L2 (3 vector arrays of dim x 128 x 8 B each)",
+                       "parallelism": f"weak: one k-block per rank x{ws}"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "kernel": "k_hv (on-the-fly multi-vector H*V)",
+                         "bytes_per_launch": bytes_per_launch,
+                         "traffic": ncu_traffic()},
+            "e2e": {"value": e2e_val, "unit": "GB/s",
+                    "h2d_bytes_per_step": pe["h2d_bytes"] / args.steps,
+                    "d2h_bytes_per_step": pe["d2h_bytes"] / args.steps},
+            "gpu_launches": prof["kernel_launches"],
+            "clocks": clk.summary(),
+        }
+        if base:
+            line["cpu_baseline"] = base
+        print(json.dumps(line))
+    eng.close()
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
+    ap.add_argument("--batch", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,334 @@
+// Exact block spectra on the GPU (diagonalize_block_exact, main.cpp:847-911).
+//
+// Every block of the list is assembled as a dense column-major Hermitian
+// matrix from its device CSR, symmetrised as (M + M^H)/2 like the
+// reference, then all matrices are diagonalised by ONE batched launch:
+// one CTA per matrix (largest first) reduces it to real symmetric
+// tridiagonal form with complex Householder reflections (trailing
+// rank-2 updates, coalesced along columns) and finds every eigenvalue
+// independently by Sturm-sequence bisection, one thread per eigenvalue,
+// which yields them sorted ascending. Eigenvalues only (jobz = 'N').
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <numeric>
+
+#include "ftlm_internal.h"
+
+namespace ftlm {
+
+namespace {
+
+constexpr int kEigThreads = 256;
+constexpr int kMaxDense = 7000;  // two complex work vectors in shared memory: 2*7000*16 B <= 227 KB
+
+__global__ void k_dense_build(int64_t n, const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
+                              const double2* __restrict__ val, const double* __restrict__ diag,
+                              double2* __restrict__ A) {
+  // row i of M -> A[i + j*n]; one thread per row keeps the entry order
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    A[i + i * n].x += diag[i];
+    for (int32_t e = rp[i]; e < rp[i + 1]; ++e) {
+      double2& a = A[i + static_cast<int64_t>(col[e]) * n];
+      a.x += val[e].x;
+      a.y += val[e].y;
+    }
+  }
+}
+
+// (M + M^H)/2 with a real diagonal (main.cpp:875-886); upper triangle
+// holds the average, the lower triangle its conjugate.
+__global__ void k_dense_herm(int64_t n, double2* __restrict__ A) {
+  for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < n * n;
+       t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t i = t % n, j = t / n;
+    if (i > j) continue;
+    if (i == j) {
+      A[i + i * n].y = 0.0;
+      continue;
+    }
+    const double2 a = A[i + j * n], b = A[j + i * n];
+    const double re = 0.5 * (a.x + b.x), im = 0.5 * (a.y - b.y);
+    A[i + j * n] = make_double2(re, im);
+    A[j + i * n] = make_double2(re, -im);
+  }
+}
+
+__device__ double block_sum(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double s = 0.0;
+  for (int w = 0; w < kEigThreads / 32; ++w) s += red[w];
+  __syncthreads();
+  return s;
+}
+
+__device__ double block_minmax(double v, double* red, bool is_max) {
+  for (int o = 16; o > 0; o >>= 1) {
+    const double t = __shfl_xor_sync(0xffffffffu, v, o);
+    v = is_max ? fmax(v, t) : fmin(v, t);
+  }
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double s = red[0];
+  for (int w = 1; w < kEigThreads / 32; ++w) s = is_max ? fmax(s, red[w]) : fmin(s, red[w]);
+  __syncthreads();
+  return s;
+}
+
+// Number of eigenvalues of the tridiagonal (d, e2 = e^2) below x.
+__device__ int sturm_count(int n, const double* d, const double* e2, double x, double pivmin) {
+  double q = d[0] - x;
+  if (fabs(q) < pivmin) q = -pivmin;
+  int cnt = q < 0.0;
+  for (int i = 1; i < n; ++i) {
+    q = d[i] - x - e2[i - 1] / q;
+    if (fabs(q) < pivmin) q = -pivmin;
+    cnt += q < 0.0;
+  }
+  return cnt;
+}
+
+// One CTA per matrix. work: per matrix 2*n doubles (d, e2) at woff.
+__global__ void __launch_bounds__(kEigThreads) k_dense_eig(int nmat, const int32_t* __restrict__ order,
+                                                          const int32_t* __restrict__ dims,
+                                                          const int64_t* __restrict__ aoff, double2* __restrict__ arena,
+                                                          const int64_t* __restrict__ eoff, double* __restrict__ evout,
+                                                          double* __restrict__ work, const int64_t* __restrict__ woff) {
+  extern __shared__ double2 sh[];
+  __shared__ double red[kEigThreads / 32];
+  for (int task = blockIdx.x; task < nmat; task += gridDim.x) {
+    const int mi = order[task];
+    const int n = dims[mi];
+    double2* A = arena + aoff[mi];
+    double* d = work + woff[mi];
+    double* e2 = d + n;
+    double2* v = sh;
+    double2* w = sh + n;
+    const int tid = threadIdx.x;
+    for (int k = 0; k + 2 < n; ++k) {
+      const int m = n - k - 1;
+      const int64_t base = (k + 1) + static_cast<int64_t>(k) * n;  // A[k+1][k]
+      double s2 = 0.0;
+      for (int i = tid; i < m; i += kEigThreads) {
+        const double2 x = A[base + i];
+        s2 += x.x * x.x + x.y * x.y;
+      }
+      const double alpha = sqrt(block_sum(s2, red));
+      if (tid == 0) d[k] = A[k + static_cast<int64_t>(k) * n].x;
+      if (alpha == 0.0) {
+        if (tid == 0) e2[k] = 0.0;
+        __syncthreads();
+        continue;
+      }
+      const double2 x0 = A[base];
+      const double ax0 = hypot(x0.x, x0.y);
+      const double phr = ax0 > 0.0 ? x0.x / ax0 : 1.0;
+      const double phi = ax0 > 0.0 ? x0.y / ax0 : 0.0;
+      for (int i = tid; i < m; i += kEigThreads) {
+        double2 x = A[base + i];
+        if (i == 0) {
+          x.x += phr * alpha;
+          x.y += phi * alpha;
+        }
+        v[i] = x;
+      }
+      const double tau = 1.0 / (alpha * (alpha + ax0));  // 2 / |v|^2
+      __syncthreads();
+      // p = tau * B v, B = A[k+1.., k+1..] (thread per row, columns in order)
+      const int64_t b0 = (k + 1) + static_cast<int64_t>(k + 1) * n;
+      double kr = 0.0;
+      for (int i = tid; i < m; i += kEigThreads) {
+        double pr = 0.0, pi = 0.0;
+        for (int j = 0; j < m; ++j) {
+          const double2 b = A[b0 + i + static_cast<int64_t>(j) * n];
+          const double2 vj = v[j];
+          pr += b.x * vj.x - b.y * vj.y;
+          pi += b.x * vj.y + b.y * vj.x;
+        }
+        pr *= tau;
+        pi *= tau;
+        w[i] = make_double2(pr, pi);
+        kr += v[i].x * pr + v[i].y * pi;  // Re(conj(v_i) p_i)
+      }
+      const double K = 0.5 * tau * block_sum(kr, red);
+      for (int i = tid; i < m; i += kEigThreads) {
+        w[i].x -= K * v[i].x;
+        w[i].y -= K * v[i].y;
+      }
+      __syncthreads();
+      // B -= v w^H + w v^H
+      for (int j = 0; j < m; ++j) {
+        const double2 vj = v[j], wj = w[j];
+        for (int i = tid; i < m; i += kEigThreads) {
+          const double2 vi = v[i], wi = w[i];
+          double2& b = A[b0 + i + static_cast<int64_t>(j) * n];
+          b.x -= (vi.x * wj.x + vi.y * wj.y) + (wi.x * vj.x + wi.y * vj.y);
+          b.y -= (vi.y * wj.x - vi.x * wj.y) + (wi.y * vj.x - wi.x * vj.y);
+        }
+      }
+      if (tid == 0) e2[k] = alpha * alpha;
+      __syncthreads();
+    }
+    if (tid == 0) {
+      if (n >= 2) {
+        d[n - 2] = A[(n - 2) + static_cast<int64_t>(n - 2) * n].x;
+        const double2 t = A[(n - 1) + static_cast<int64_t>(n - 2) * n];
+        e2[n - 2] = t.x * t.x + t.y * t.y;
+      }
+      d[n - 1] = A[(n - 1) + static_cast<int64_t>(n - 1) * n].x;
+      e2[n - 1] = 0.0;
+    }
+    __syncthreads();
+    // Gershgorin interval and bisection
+    double lo = DBL_MAX, hi = -DBL_MAX, emax = 0.0;
+    for (int i = tid; i < n; i += kEigThreads) {
+      const double el = i > 0 ? sqrt(e2[i - 1]) : 0.0;
+      const double er = i + 1 < n ? sqrt(e2[i]) : 0.0;
+      lo = fmin(lo, d[i] - el - er);
+      hi = fmax(hi, d[i] + el + er);
+      emax = fmax(emax, e2[i]);
+    }
+    lo = block_minmax(lo, red, false);
+    hi = block_minmax(hi, red, true);
+    emax = block_minmax(emax, red, true);
+    const double pivmin = DBL_MIN * fmax(1.0, emax);
+    const double span = fmax(fabs(lo), fabs(hi));
+    lo -= 4.0 * DBL_EPSILON * span + pivmin;
+    hi += 4.0 * DBL_EPSILON * span + pivmin;
+    double* ev = evout + eoff[mi];
+    for (int j = tid; j < n; j += kEigThreads) {
+      double a = lo, b = hi;
+      for (int it = 0; it < 128; ++it) {
+        const double mid = 0.5 * (a + b);
+        if (mid <= a || mid >= b) break;
+        if (b - a <= 2.0 * DBL_EPSILON * fmax(fabs(a), fabs(b))) break;
+        if (sturm_count(n, d, e2, mid, pivmin) > j) b = mid;
+        else a = mid;
+      }
+      ev[j] = 0.5 * (a + b);
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace
+
+void run_exact_blocks(Ctx& c, const std::vector<std::pair<int, int>>& blocks) {
+  struct Item {
+    int mx, my;
+    int64_t n, aoff, eoff, woff;
+  };
+  std::vector<Item> items;
+  int64_t asz = 0, wsz = 0;
+  // dimensions first (tables per block are rebuilt below)
+  for (const auto& b : blocks) {
+    block_prepare(c, b.first, b.second);
+    const int64_t n = c.blk.dim;
+    if (n <= 0) continue;
+    if (n > kMaxDense) throw Error(FTLM_ERR_CAPACITY, "block too large for the dense exact solver: " + std::to_string(n));
+    items.push_back({b.first, b.second, n, asz, 0, wsz});
+    asz += n * n;
+    wsz += 2 * n;
+  }
+  if (items.empty()) return;
+  c.dense_arena.ensure(sizeof(double2) * asz);
+  c.dense_out.ensure(sizeof(double) * wsz);
+  FTLM_CUDA(cudaMemsetAsync(c.dense_arena.p, 0, sizeof(double2) * asz, c.stream));
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (c.timing) {
+    FTLM_CUDA(cudaEventCreate(&e0));
+    FTLM_CUDA(cudaEventCreate(&e1));
+    FTLM_CUDA(cudaEventRecord(e0, c.stream));
+  }
+  DBuf rp, cl, vl, dg;
+  for (Item& it : items) {
+    block_prepare(c, it.mx, it.my);
+    block_csr_device(c, rp, cl, vl, dg);
+    double2* A = c.dense_arena.as<double2>() + it.aoff;
+    const int g1 = static_cast<int>(std::min<int64_t>((it.n + 127) / 128, 4096));
+    k_dense_build<<<g1, 128, 0, c.stream>>>(it.n, rp.as<int32_t>(), cl.as<int32_t>(), vl.as<double2>(), dg.as<double>(), A);
+    const int g2 = static_cast<int>(std::min<int64_t>((it.n * it.n + 255) / 256, 4096));
+    k_dense_herm<<<g2, 256, 0, c.stream>>>(it.n, A);
+    FTLM_LAUNCH_CHECK();
+    c.prof.kernel_launches += 2;
+    it.eoff = spectra_alloc(c, it.n);
+    // dense_build reads rp/cl/vl before they are rebuilt for the next block
+    FTLM_CUDA(cudaStreamSynchronize(c.stream));
+  }
+  rp.release();
+  cl.release();
+  vl.release();
+  dg.release();
+  if (c.timing) {
+    FTLM_CUDA(cudaEventRecord(e1, c.stream));
+    FTLM_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    FTLM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    c.prof.dense_ms += ms;
+    FTLM_CUDA(cudaEventRecord(e0, c.stream));
+  }
+  // largest first; one CTA per matrix
+  std::vector<int32_t> order(items.size()), dims(items.size());
+  std::vector<int64_t> aoff(items.size()), eoff(items.size()), woff(items.size());
+  int64_t nmax = 0;
+  for (size_t i = 0; i < items.size(); ++i) {
+    dims[i] = static_cast<int32_t>(items[i].n);
+    aoff[i] = items[i].aoff;
+    eoff[i] = items[i].eoff;
+    woff[i] = items[i].woff;
+    nmax = std::max(nmax, items[i].n);
+  }
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return dims[a] > dims[b]; });
+  const size_t nb = items.size();
+  const size_t i32bytes = ((sizeof(int32_t) * 2 * nb + 7) / 8) * 8;  // int64 arrays stay 8-byte aligned
+  c.dense_meta.ensure(i32bytes + sizeof(int64_t) * 3 * nb);
+  int32_t* d_order = c.dense_meta.as<int32_t>();
+  int32_t* d_dims = d_order + nb;
+  int64_t* d_aoff = reinterpret_cast<int64_t*>(c.dense_meta.as<char>() + i32bytes);
+  int64_t* d_eoff = d_aoff + nb;
+  int64_t* d_woff = d_eoff + nb;
+  FTLM_CUDA(cudaMemcpyAsync(d_order, order.data(), sizeof(int32_t) * nb, cudaMemcpyHostToDevice, c.stream));
+  FTLM_CUDA(cudaMemcpyAsync(d_dims, dims.data(), sizeof(int32_t) * nb, cudaMemcpyHostToDevice, c.stream));
+  FTLM_CUDA(cudaMemcpyAsync(d_aoff, aoff.data(), sizeof(int64_t) * nb, cudaMemcpyHostToDevice, c.stream));
+  FTLM_CUDA(cudaMemcpyAsync(d_eoff, eoff.data(), sizeof(int64_t) * nb, cudaMemcpyHostToDevice, c.stream));
+  FTLM_CUDA(cudaMemcpyAsync(d_woff, woff.data(), sizeof(int64_t) * nb, cudaMemcpyHostToDevice, c.stream));
+  c.prof.h2d_bytes += static_cast<int64_t>(nb) * 32;
+  const size_t smem = sizeof(double2) * 2 * static_cast<size_t>(nmax);
+  if (smem > 48 * 1024)
+    FTLM_CUDA(cudaFuncSetAttribute(k_dense_eig, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+  const int grid = static_cast<int>(std::min<size_t>(nb, static_cast<size_t>(c.sm_count) * 4));
+  k_dense_eig<<<grid, kEigThreads, smem, c.stream>>>(static_cast<int>(nb), d_order, d_dims, d_aoff,
+                                                     c.dense_arena.as<double2>(), d_eoff, c.spectra.as<double>(),
+                                                     c.dense_out.as<double>(), d_woff);
+  FTLM_LAUNCH_CHECK();
+  c.prof.kernel_launches += 1;
+  if (c.timing) {
+    FTLM_CUDA(cudaEventRecord(e1, c.stream));
+    FTLM_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    FTLM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    c.prof.eig_ms += ms;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
+  FTLM_CUDA(cudaStreamSynchronize(c.stream));
+  for (const Item& it : items) {
+    Spectrum s;
+    s.ev_off = it.eoff;
+    s.w_off = -1;
+    s.count = it.n;
+    s.exact = true;
+    s.prefactor = 1.0;
+    s.particles = c.sec.n_up + c.sec.n_dn;
+    s.dim = it.n;
+    c.spec[{it.mx, it.my}] = s;
+  }
+}
+
+}  // namespace ftlm

@@ -1,0 +1,218 @@
+// Internal host-side structures of the B200 FTLM engine (not part of the ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/ftlm_gpu.h"
+#include "ftlm_device.cuh"
+
+namespace ftlm {
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define FTLM_CUDA(call)                                                                  \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess)                                                               \
+      throw ::ftlm::Error(FTLM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+#define FTLM_LAUNCH_CHECK() FTLM_CUDA(cudaGetLastError())
+
+// Grow-only device buffer owned by a context.
+struct DBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  void ensure(size_t bytes) {
+    if (bytes <= cap) return;
+    if (p) FTLM_CUDA(cudaFree(p));
+    p = nullptr;
+    cap = 0;
+    if (bytes == 0) return;
+    FTLM_CUDA(cudaMalloc(&p, bytes));
+    cap = bytes;
+  }
+  template <typename T>
+  T* as() const { return static_cast<T*>(p); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
+
+// Translation-orbit tables of one (N_up, N_down) sector.
+//
+// Representatives are the lexicographic minima of (up, down) orbits
+// (main.cpp:643-675 keeps the first member met in an (up, down) ascending
+// sweep). Hence the representative's up word is the minimum of its up
+// orbit ("up representative" ur), and its down word is minimal among the
+// images of the down word under the stabiliser H of ur. Up representatives
+// with equal (H, sign character of H on the up word) form a class; each
+// non-trivial class owns a table over all down words. Parents are ordered
+// by (ur, canonical down), which is the reference's parent order.
+struct SectorTables {
+  int n_up = -1, n_dn = -1;
+  int64_t c_up = 0, c_dn = 0, full_dim = 0, parents = 0;
+  int64_t nur = 0;      // number of up representatives
+  int nclass = 0;       // classes; class 0 is the trivial stabiliser
+  std::vector<uint64_t> cls_stab, cls_sig;   // per class: H mask, sign mask
+  std::vector<int64_t> cls_ncanon;           // canonical downs per class
+  std::vector<uint16_t> h_ur_class;          // host copy of ur -> class
+  DBuf ups, dns;         // W[c_up], W[c_dn] bit words in ascending order
+  DBuf up_info;          // uint64[c_up]
+  DBuf ur_bits;          // W[nur]
+  DBuf ur_class;         // uint16[nur]
+  DBuf ur_poff;          // int64[nur+1] parent offsets
+  // per non-trivial class c (index c-1), over all down ranks
+  DBuf d_star;           // uint32[(nclass-1)*c_dn] rank of the canonical image
+  DBuf d_hs;             // uint16[(nclass-1)*c_dn] h | sign<<8 (T_h d* = d)
+  DBuf d_stab, d_chi;    // uint64[(nclass-1)*c_dn] for canonical words
+  DBuf d_cidx;           // int32[(nclass-1)*c_dn] canonical index (scan)
+  DBuf canon;            // int32[(nclass-1)*c_dn] 1 for canonical words
+  DBuf tmp_a, tmp_b, tmp_c, tmp_d, tmp_e;  // build scratch
+};
+
+// Tables of one momentum block (mx, my) of the prepared sector.
+struct BlockTables {
+  int mx = -1, my = -1;
+  int64_t dim = 0;
+  std::vector<int64_t> cls_nact;  // active canonical downs per class
+  DBuf act;       // int32[(nclass-1)*c_dn] active index of canonical words (-1)
+  DBuf act_list;  // uint32[(nclass-1)*c_dn] ranks of active canonical words
+  DBuf aoff;      // int64[nur+1] active row offsets
+  DBuf dtab;      // uint64[(nclass-1)*c_dn] packed lookup entries
+  DBuf row_meta;  // uint32[dim]: ur | (deg-1)<<26
+  DBuf row_dn;    // W[dim]
+  double phase_re[64], phase_im[64];
+};
+
+// Everything the H*V / CSR kernels need about one block.
+template <typename W>
+struct BlockView {
+  const uint64_t* up_info;
+  const W* ur_bits;
+  const uint16_t* ur_class;
+  const int64_t* aoff;
+  const uint64_t* dtab;
+  const uint32_t* row_meta;
+  const W* row_dn;
+  int64_t c_dn;
+  int64_t dim;
+  int n_up, n_dn;
+  double phase_re[64], phase_im[64];
+};
+
+// Device-resident spectrum of one block.
+struct Spectrum {
+  int64_t ev_off = 0;  // eigenvalues at spectra[ev_off .. ev_off+count)
+  int64_t w_off = -1;  // weights at spectra[w_off ..), -1 for exact blocks
+  int64_t count = 0;   // number of eigenvalues
+  bool exact = false;
+  double prefactor = 1.0;
+  int particles = 0;
+  int64_t dim = 0;
+};
+
+struct Profile {
+  double hv_ms = 0.0;       // summed CUDA-event time of H*V launches
+  int64_t hv_launches = 0;
+  double hv_bytes = 0.0;    // algorithmic bytes of those launches
+  double update_ms = 0.0;
+  int64_t update_launches = 0;
+  double eig_ms = 0.0;
+  double dense_ms = 0.0;
+  double thermo_ms = 0.0;
+  double sector_ms = 0.0;
+  double block_ms = 0.0;
+  int64_t kernel_launches = 0;
+  int64_t h2d_bytes = 0, d2h_bytes = 0;
+};
+
+struct Ctx {
+  ftlm_model model{};
+  ftlm_run_opts opts{};
+  Geom geom{};
+  bool wide = false;  // 64-bit spin words (more than 32 sites)
+  int device = 0;
+  int sm_count = 148;
+  cudaStream_t stream = nullptr;
+  std::string last_error;
+  DBuf binom;         // uint64 [65*65]
+  DBuf binom32;       // uint32 [65*65]
+  SectorTables sec;
+  BlockTables blk;
+  // Lanczos work space
+  DBuf vec_a, vec_b, vec_h, partial, lz_alpha, lz_beta, lz_scale, lz_state, host_start;
+  DBuf ritz_tmp, scan_tmp;
+  // exact batch
+  DBuf dense_arena, dense_meta, dense_out;
+  // spectra of the current sector's blocks (device arena)
+  DBuf spectra;
+  int64_t spectra_used = 0;
+  std::map<std::pair<int, int>, Spectrum> spec;
+  // thermo
+  int nbeta = 0, nmu = 0;
+  DBuf th_beta, th_mu, th_state;  // state: [4][nbeta][nmu] emin, z, n, n2
+  // instrumentation
+  bool timing = false;
+  Profile prof;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // last Lanczos run (debug readback)
+  int last_kdim = 0, last_nv = 0;
+};
+
+// ---- launchers implemented in the .cu files
+void sector_prepare(Ctx& c, int n_up, int n_dn);
+void block_prepare(Ctx& c, int mx, int my);
+int64_t block_dim_only(Ctx& c, int mx, int my);
+void debug_parents(Ctx& c, uint64_t* up, uint64_t* dn, int32_t* deg, double* diag);
+void debug_relations(Ctx& c, int32_t* parent, int32_t* shift, int32_t* sign);
+void block_csr(Ctx& c, std::vector<int32_t>& row_ptr, std::vector<int32_t>& col,
+               std::vector<double>& val, std::vector<double>& diag);
+// Device CSR of the prepared block (reference entry order); returns nnz.
+int64_t block_csr_device(Ctx& c, DBuf& row_ptr, DBuf& col, DBuf& val, DBuf& diag);
+// H*V of the prepared block on device arrays [dim][nv] complex (FP64 or FP32).
+void hv_apply(Ctx& c, const void* in, void* out, int nv, bool fp32, const double* scale_dev,
+              double* partial_dev, int nblocks_hint);
+int hv_grid(Ctx& c, int nv, bool fp32);
+BlockView<uint32_t> view32(Ctx& c);
+BlockView<uint64_t> view64(Ctx& c);
+
+// Lanczos over the prepared block; results stored as a Spectrum.
+void run_ftlm_block(Ctx& c, int n_up, int n_dn, int mx, int my, Spectrum& out,
+                    const double* host_start /* [R][dim] complex or null */,
+                    std::vector<double>* alpha_out, std::vector<double>* beta_out,
+                    std::vector<int32_t>* steps_out);
+// Exact spectra of several blocks of the prepared sector (one batched launch).
+void run_exact_blocks(Ctx& c, const std::vector<std::pair<int, int>>& blocks);
+// Thermo
+void thermo_configure(Ctx& c, int nbeta, const double* beta, int nmu, const double* mu);
+void thermo_accumulate(Ctx& c, const Spectrum& s);
+void thermo_accumulate_host(Ctx& c, const double* ev, const double* w, int64_t count, double pref, int particles);
+void thermo_read(Ctx& c, double* emin, double* z, double* n, double* n2);
+
+// Seeds and reference start vectors (main.cpp:514-533, 1015-1025)
+uint64_t block_seed(uint64_t seed, int n_up, int n_dn, int mx, int my);
+void reference_start_vectors(uint64_t bseed, int sample0, int nva, int64_t dim, double* out);
+// Nonzero-amplitude hops with active targets in the prepared block (the
+// h_nz * dim of the H*V byte model).
+int64_t block_nonzero_hops(Ctx& c);
+
+// Spectra arena
+int64_t spectra_alloc(Ctx& c, int64_t count);  // returns offset (doubles) of 2*count slots
+void spectra_reset(Ctx& c);
+
+// Scan helpers (exclusive, in place on device, returns total)
+int64_t scan_excl_i32_to_i64(Ctx& c, const int32_t* flags, int64_t* out, int64_t n);
+
+}  // namespace ftlm

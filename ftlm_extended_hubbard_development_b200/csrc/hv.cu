@@ -1,0 +1,567 @@
+// Momentum-block Hamiltonian on the GPU.
+//
+// Two forms of H of block (mx, my):
+//  * block_csr_device: explicit CSR in the reference's entry order
+//    (build_momentum_block, main.cpp:779-804), for parity checks and the
+//    dense exact path;
+//  * k_hv: on-the-fly multi-vector H*V (apply_hamiltonian, main.cpp:833-845,
+//    applied to nv vectors at once). No matrix is stored. Each warp owns a
+//    row: its lanes enumerate the row's hops into a shared-memory queue,
+//    resolve one hop target each (rank -> orbit table -> column, sign, phase),
+//    then broadcast (column, coefficient) by warp shuffle while groups of
+//    lanes gather the target rows of all nv vectors with 16-byte loads.
+//    Vector layout is [dim][nv] so one gathered row is nv*sizeof(complex)
+//    contiguous bytes.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "ftlm_internal.h"
+
+namespace ftlm {
+
+namespace {
+
+int grid_for(int64_t n, int threads) {
+  return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>((n + threads - 1) / threads, 1 << 20)));
+}
+
+// Resolve a hop target (tu, td) to its block column, translation shift,
+// sign parity and orbit stabiliser size. Returns false when the target's
+// orbit is inactive in this block (main.cpp:790-793).
+template <typename W, typename R>
+__device__ __forceinline__ bool resolve(W tu, W td, bool up_hop, uint32_t ur_src, const BlockView<W>& v,
+                                        const Geom& g, const R* binom, int64_t& col, int& shift, int& sgn,
+                                        int& deg) {
+  uint32_t ur = ur_src;
+  int g0 = 0;
+  int s = 0;
+  W dd = td;
+  if (up_hop) {
+    const uint64_t info = __ldg(v.up_info + rank_of<W, R>(tu, binom));
+    ur = static_cast<uint32_t>(info);
+    g0 = static_cast<int>((info >> 32) & 0xFF);
+    s = static_cast<int>((info >> 40) & 1);
+    if (g0) {
+      int p;
+      const int ng = shift_neg(g0, g);
+      dd = translate(td, shift_dx(ng, g), shift_dy(ng, g), g, &p);
+      s ^= p;
+    }
+  }
+  const int cls = __ldg(v.ur_class + ur);
+  const int64_t rd = static_cast<int64_t>(rank_of<W, R>(dd, binom));
+  int64_t a = rd;
+  int h = 0;
+  deg = 1;
+  if (cls != 0) {
+    const uint64_t e = __ldg(v.dtab + static_cast<int64_t>(cls - 1) * v.c_dn + rd);
+    a = static_cast<int32_t>(static_cast<uint32_t>(e));
+    if (a < 0) return false;
+    h = static_cast<int>((e >> 32) & 0xFF);
+    s ^= static_cast<int>((e >> 40) & 1);
+    deg = static_cast<int>((e >> 48) & 0xFF);
+  }
+  shift = h ? shift_add(g0, h, g) : g0;
+  sgn = s;
+  col = __ldg(v.aoff + ur) + a;
+  return true;
+}
+
+template <typename W>
+struct CsrParams {
+  Geom g;
+  BlockView<W> v;
+};
+
+// One thread per row, hops in reference order: up spin first, occupied
+// source sites ascending, directions 0..7, zero-amplitude hops included.
+template <typename W>
+__global__ void k_csr(const __grid_constant__ CsrParams<W> P, const uint64_t* __restrict__ binom, int fill,
+                      int32_t* __restrict__ counts, const int64_t* __restrict__ row_ptr, int32_t* __restrict__ col,
+                      double* __restrict__ val, double* __restrict__ diag) {
+  const Geom& g = P.g;
+  const BlockView<W>& v = P.v;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < v.dim;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const uint32_t meta = v.row_meta[i];
+    const uint32_t ur = meta & 0x3FFFFFFu;
+    const int deg_s = static_cast<int>(meta >> 26) + 1;
+    const W u = v.ur_bits[ur];
+    const W d = v.row_dn[i];
+    int64_t pos = fill == 1 ? row_ptr[i] : 0;  // row_ptr exists only in the fill pass
+    int cnt = 0;
+    for (int spin = 0; spin < 2; ++spin) {
+      const W bits = spin ? d : u;
+      for (W m = bits; m; m &= m - 1) {
+        const int from = ctz(m);
+        for (int dir = 0; dir < 8; ++dir) {
+          const int to = g.nb[from][dir];
+          if ((bits >> to) & 1) continue;
+          if (fill == 2 && g.amp_re[dir] == 0.0 && g.amp_im[dir] == 0.0) continue;
+          const W moved = bits ^ (static_cast<W>(1) << from) ^ (static_cast<W>(1) << to);
+          int64_t c;
+          int shift, sgn, deg_t;
+          if (!resolve<W, uint64_t>(spin ? u : moved, spin ? moved : d, spin == 0, ur, v, g, binom, c, shift,
+                                    sgn, deg_t))
+            continue;
+          if (fill == 1) {
+            const int p = jw_parity(bits, from, to) ^ sgn;
+            // ((amp * sign) * phase) * ratio, the operation order of main.cpp:794-797
+            const double ar = p ? -g.amp_re[dir] : g.amp_re[dir];
+            const double ai = p ? -g.amp_im[dir] : g.amp_im[dir];
+            const double pr = v.phase_re[shift], pi = v.phase_im[shift];
+            const double re = __dsub_rn(__dmul_rn(ar, pr), __dmul_rn(ai, pi));
+            const double im = __dadd_rn(__dmul_rn(ar, pi), __dmul_rn(ai, pr));
+            const double ratio = __ddiv_rn(g.sqrt_deg[deg_t], g.sqrt_deg[deg_s]);
+            col[pos] = static_cast<int32_t>(c);
+            val[2 * pos] = __dmul_rn(re, ratio);
+            val[2 * pos + 1] = __dmul_rn(im, ratio);
+            ++pos;
+          }
+          ++cnt;
+        }
+      }
+    }
+    if (fill == 1) diag[i] = diag_energy(u, d, g);
+    else counts[i] = cnt;
+  }
+}
+
+__global__ void k_i64_to_i32(const int64_t* __restrict__ in, int32_t* __restrict__ out, int64_t n) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    out[i] = static_cast<int32_t>(in[i]);
+}
+
+// ------------------------------------------------------------ H*V kernel
+
+template <typename T>
+struct CT;  // 16-byte chunk type and complex-per-chunk count
+template <>
+struct CT<float> {
+  using V = float4;
+  static constexpr int VPL = 2;
+};
+template <>
+struct CT<double> {
+  using V = double2;
+  static constexpr int VPL = 1;
+};
+
+template <typename W>
+struct HvParams {
+  Geom g;
+  BlockView<W> v;
+};
+
+constexpr int kHvThreads = 256;
+constexpr int kHvWarps = kHvThreads / 32;
+// hop codes per warp: 8 directions * (N_up + N_down) <= 16 * bits per word
+template <typename W>
+constexpr int queue_len() { return 16 * static_cast<int>(sizeof(W)) * 8; }
+
+// k-th (0-based) set bit of x.
+template <typename W>
+__device__ __forceinline__ int kth_bit(W x, int k) {
+  int pos = 0;
+#pragma unroll
+  for (int w = sizeof(W) * 4; w >= 1; w >>= 1) {
+    const W lowmask = static_cast<W>((static_cast<W>(1) << w) - 1);
+    const int c = popc(static_cast<W>(x & lowmask));
+    if (k >= c) {
+      k -= c;
+      x >>= w;
+      pos += w;
+    }
+  }
+  return pos;
+}
+
+template <typename T>
+__device__ __forceinline__ void cfma(typename CT<T>::V& acc, T cr, T ci, const typename CT<T>::V& x);
+
+template <>
+__device__ __forceinline__ void cfma<float>(float4& acc, float cr, float ci, const float4& x) {
+  acc.x = fmaf(cr, x.x, fmaf(-ci, x.y, acc.x));
+  acc.y = fmaf(cr, x.y, fmaf(ci, x.x, acc.y));
+  acc.z = fmaf(cr, x.z, fmaf(-ci, x.w, acc.z));
+  acc.w = fmaf(cr, x.w, fmaf(ci, x.z, acc.w));
+}
+template <>
+__device__ __forceinline__ void cfma<double>(double2& acc, double cr, double ci, const double2& x) {
+  acc.x = fma(cr, x.x, fma(-ci, x.y, acc.x));
+  acc.y = fma(cr, x.y, fma(ci, x.x, acc.y));
+}
+
+__device__ __forceinline__ float4 shfl_xor_v(float4 a, int m) {
+  a.x = __shfl_xor_sync(0xffffffffu, a.x, m);
+  a.y = __shfl_xor_sync(0xffffffffu, a.y, m);
+  a.z = __shfl_xor_sync(0xffffffffu, a.z, m);
+  a.w = __shfl_xor_sync(0xffffffffu, a.w, m);
+  return a;
+}
+__device__ __forceinline__ double2 shfl_xor_v(double2 a, int m) {
+  a.x = __shfl_xor_sync(0xffffffffu, a.x, m);
+  a.y = __shfl_xor_sync(0xffffffffu, a.y, m);
+  return a;
+}
+__device__ __forceinline__ void vzero(float4& a) { a = make_float4(0.f, 0.f, 0.f, 0.f); }
+__device__ __forceinline__ void vzero(double2& a) { a = make_double2(0.0, 0.0); }
+__device__ __forceinline__ void vadd(float4& a, const float4& b) {
+  a.x += b.x; a.y += b.y; a.z += b.z; a.w += b.w;
+}
+__device__ __forceinline__ void vadd(double2& a, const double2& b) {
+  a.x += b.x; a.y += b.y;
+}
+
+// y = s_v * (diag * x + acc) per complex element; returns Re(conj(s_v x) y)
+// summed per element into dot[e].
+__device__ __forceinline__ float4 finish_row(const float4& x, const float4& acc, double diag, const double* s,
+                                             double* dot) {
+  const float df = static_cast<float>(diag);
+  float4 y;
+  y.x = fmaf(df, x.x, acc.x);
+  y.y = fmaf(df, x.y, acc.y);
+  y.z = fmaf(df, x.z, acc.z);
+  y.w = fmaf(df, x.w, acc.w);
+  y.x = static_cast<float>(s[0] * y.x);
+  y.y = static_cast<float>(s[0] * y.y);
+  y.z = static_cast<float>(s[1] * y.z);
+  y.w = static_cast<float>(s[1] * y.w);
+  dot[0] += s[0] * (static_cast<double>(x.x) * y.x + static_cast<double>(x.y) * y.y);
+  dot[1] += s[1] * (static_cast<double>(x.z) * y.z + static_cast<double>(x.w) * y.w);
+  return y;
+}
+__device__ __forceinline__ double2 finish_row(const double2& x, const double2& acc, double diag, const double* s,
+                                              double* dot) {
+  double2 y;
+  y.x = s[0] * fma(diag, x.x, acc.x);
+  y.y = s[0] * fma(diag, x.y, acc.y);
+  dot[0] += s[0] * (x.x * y.x + x.y * y.y);
+  return y;
+}
+
+// H*V over all rows of the block. in/out: [dim][NV] complex T as 16-byte
+// chunks. scale[v] multiplies the result of vector v (Lanczos vectors are
+// stored unnormalised). partial[block][NV] receives Re<s*in, out> sums
+// (deterministic order), or nothing when partial == nullptr.
+template <typename W, typename R, typename T, int NV>
+__global__ void __launch_bounds__(kHvThreads) k_hv(const __grid_constant__ HvParams<W> P,
+                                                   const typename CT<T>::V* __restrict__ in,
+                                                   typename CT<T>::V* __restrict__ out,
+                                                   const double* __restrict__ scale, double* __restrict__ partial,
+                                                   const R* __restrict__ gbinom) {
+  using V = typename CT<T>::V;
+  constexpr int VPL = CT<T>::VPL;
+  constexpr int CPR = NV / VPL;                 // 16-byte chunks per row
+  constexpr int G = CPR < 32 ? CPR : 32;        // lanes per gathered row
+  constexpr int LPL = CPR / G;                  // chunks per lane
+  constexpr int HPAR = 32 / G;                  // rows gathered in parallel
+  constexpr bool kSmemBinom = sizeof(W) == 4;   // 64-bit words read C(n,k) from global/L1
+  constexpr int kQ = queue_len<W>();
+
+  __shared__ R s_binom[kSmemBinom ? 32 * 65 : 1];
+  __shared__ int8_t s_nb[64][8];
+  __shared__ double s_ph[2][64];
+  __shared__ double s_amp[2][8];
+  __shared__ double s_sq[65];
+  __shared__ uint16_t s_q[kHvWarps][kQ];
+  __shared__ double s_dot[kHvWarps][NV];
+
+  const Geom& g = P.g;
+  const BlockView<W>& v = P.v;
+  const int tid = threadIdx.x;
+  if (kSmemBinom)
+    for (int i = tid; i < 32 * 65; i += kHvThreads) s_binom[i] = gbinom[i];
+  const R* binom = kSmemBinom ? s_binom : gbinom;
+  for (int i = tid; i < 64 * 8; i += kHvThreads) s_nb[i / 8][i % 8] = g.nb[i / 8][i % 8];
+  for (int i = tid; i < 64; i += kHvThreads) {
+    s_ph[0][i] = v.phase_re[i];
+    s_ph[1][i] = v.phase_im[i];
+  }
+  if (tid < 8) {
+    s_amp[0][tid] = g.amp_re[tid];
+    s_amp[1][tid] = g.amp_im[tid];
+  }
+  if (tid < 65) s_sq[tid] = g.sqrt_deg[tid];
+  __syncthreads();
+
+  const int lane = tid & 31;
+  const int wid = tid >> 5;
+  const int grp = lane / G;
+  const int sub = lane % G;
+  uint16_t* queue = s_q[wid];
+
+  double sc[LPL][VPL];
+  double dot[LPL][VPL];
+#pragma unroll
+  for (int l = 0; l < LPL; ++l)
+#pragma unroll
+    for (int e = 0; e < VPL; ++e) {
+      sc[l][e] = scale ? scale[(l * G + sub) * VPL + e] : 1.0;
+      dot[l][e] = 0.0;
+    }
+
+  const int nsite = v.n_up + v.n_dn;
+  const int64_t nwarps = static_cast<int64_t>(gridDim.x) * kHvWarps;
+  for (int64_t row = static_cast<int64_t>(blockIdx.x) * kHvWarps + wid; row < v.dim; row += nwarps) {
+    const uint32_t meta = __ldg(v.row_meta + row);
+    const uint32_t ur = meta & 0x3FFFFFFu;
+    const int deg_s = static_cast<int>(meta >> 26) + 1;
+    const W u = __ldg(v.ur_bits + ur);
+    const W d = __ldg(v.row_dn + row);
+    const double inv_s = 1.0 / s_sq[deg_s];
+
+    // 1) hop queue: lane k handles the k-th occupied (spin, site) pair
+    int total = 0;
+    for (int k0 = 0; k0 < nsite; k0 += 32) {
+      const int k = k0 + lane;
+      uint32_t dm = 0;
+      int spin = 0, from = 0;
+      if (k < nsite) {
+        spin = k >= v.n_up;
+        const W bits = spin ? d : u;
+        from = kth_bit(bits, spin ? k - v.n_up : k);
+        for (int j = 0; j < g.ndir; ++j) {
+          const int to = s_nb[from][g.dirs[j]];
+          if (!((bits >> to) & 1)) dm |= 1u << j;
+        }
+      }
+      const int cnt = __popc(dm);
+      int incl = cnt;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+      }
+      int pos = total + incl - cnt;
+      for (uint32_t m = dm; m; m &= m - 1) {
+        const int j = __ffs(m) - 1;
+        queue[pos++] = static_cast<uint16_t>((spin << 9) | (from << 3) | g.dirs[j]);
+      }
+      total += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    __syncwarp();
+
+    // 2) resolve 32 hops at a time, gather their rows
+    V acc[LPL];
+#pragma unroll
+    for (int l = 0; l < LPL; ++l) vzero(acc[l]);
+    for (int b = 0; b < total; b += 32) {
+      const int q = b + lane;
+      int64_t col = -1;
+      T cr = 0, ci = 0;
+      if (q < total) {
+        const int code = queue[q];
+        const int spin = code >> 9, from = (code >> 3) & 63, dir = code & 7;
+        const int to = s_nb[from][dir];
+        const W bits = spin ? d : u;
+        const W moved = bits ^ (static_cast<W>(1) << from) ^ (static_cast<W>(1) << to);
+        int shift, sgn, deg_t;
+        if (resolve<W, R>(spin ? u : moved, spin ? moved : d, spin == 0, ur, v, g, binom, col, shift, sgn, deg_t)) {
+          const int p = jw_parity(bits, from, to) ^ sgn;
+          const double ar = p ? -s_amp[0][dir] : s_amp[0][dir];
+          const double ai = p ? -s_amp[1][dir] : s_amp[1][dir];
+          const double pr = s_ph[0][shift], pi = s_ph[1][shift];
+          const double ratio = s_sq[deg_t] * inv_s;
+          cr = static_cast<T>((ar * pr - ai * pi) * ratio);
+          ci = static_cast<T>((ar * pi + ai * pr) * ratio);
+        }
+      }
+      const int nb = min(32, total - b);
+      for (int j = 0; j < nb; j += HPAR) {
+        const int src = (j + grp) & 31;
+        const int64_t c = __shfl_sync(0xffffffffu, col, src);
+        const T r = __shfl_sync(0xffffffffu, cr, src);
+        const T i = __shfl_sync(0xffffffffu, ci, src);
+        if (j + grp < nb && c >= 0) {
+          const V* rowp = in + c * CPR;
+#pragma unroll
+          for (int l = 0; l < LPL; ++l) {
+            const V x = __ldg(rowp + l * G + sub);
+            cfma<T>(acc[l], r, i, x);
+          }
+        }
+      }
+    }
+    __syncwarp();
+    // 3) fold the HPAR partial sums
+#pragma unroll
+    for (int o = G; o < 32; o <<= 1)
+#pragma unroll
+      for (int l = 0; l < LPL; ++l) vadd(acc[l], shfl_xor_v(acc[l], o));
+    // 4) own-row diagonal term, scale, store, Lanczos dot
+    if (grp == 0) {
+      const double diag = diag_energy(u, d, g);
+#pragma unroll
+      for (int l = 0; l < LPL; ++l) {
+        const V x = __ldg(in + row * CPR + l * G + sub);
+        out[row * CPR + l * G + sub] = finish_row(x, acc[l], diag, sc[l], dot[l]);
+      }
+    }
+  }
+
+  if (partial) {
+    if (grp == 0) {
+#pragma unroll
+      for (int l = 0; l < LPL; ++l)
+#pragma unroll
+        for (int e = 0; e < VPL; ++e) s_dot[wid][(l * G + sub) * VPL + e] = dot[l][e];
+    }
+    __syncthreads();
+    for (int vv = tid; vv < NV; vv += kHvThreads) {
+      double s = 0.0;
+      for (int w = 0; w < kHvWarps; ++w) s += s_dot[w][vv];
+      partial[static_cast<int64_t>(blockIdx.x) * NV + vv] = s;
+    }
+  }
+}
+
+template <typename W, typename R, typename T, int NV>
+void launch_hv_t(Ctx& c, const void* in, void* out, const double* scale, double* partial, int grid) {
+  if (grid < 0) {  // occupancy query: CTAs resident per SM
+    static int occ = 0;
+    if (!occ) {
+      FTLM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_hv<W, R, T, NV>, kHvThreads, 0));
+      occ = std::max(occ, 1);
+    }
+    *static_cast<int*>(out) = occ;
+    return;
+  }
+  HvParams<W> P;
+  P.g = c.geom;
+  if constexpr (sizeof(W) == 4) P.v = view32(c);
+  else P.v = view64(c);
+  using V = typename CT<T>::V;
+  const R* gb = sizeof(R) == 4 ? reinterpret_cast<const R*>(c.binom32.p) : reinterpret_cast<const R*>(c.binom.p);
+  k_hv<W, R, T, NV><<<grid, kHvThreads, 0, c.stream>>>(P, static_cast<const V*>(in), static_cast<V*>(out), scale,
+                                                       partial, gb);
+}
+
+template <typename W, typename R, typename T>
+void launch_hv_nv(Ctx& c, const void* in, void* out, int nv, const double* scale, double* partial, int grid) {
+  switch (nv) {
+    case 1:
+      if constexpr (sizeof(T) == 8) { launch_hv_t<W, R, T, 1>(c, in, out, scale, partial, grid); return; }
+      break;
+    case 2: launch_hv_t<W, R, T, 2>(c, in, out, scale, partial, grid); return;
+    case 4: launch_hv_t<W, R, T, 4>(c, in, out, scale, partial, grid); return;
+    case 8: launch_hv_t<W, R, T, 8>(c, in, out, scale, partial, grid); return;
+    case 16: launch_hv_t<W, R, T, 16>(c, in, out, scale, partial, grid); return;
+    case 32: launch_hv_t<W, R, T, 32>(c, in, out, scale, partial, grid); return;
+    case 64: launch_hv_t<W, R, T, 64>(c, in, out, scale, partial, grid); return;
+    case 128: launch_hv_t<W, R, T, 128>(c, in, out, scale, partial, grid); return;
+    default: break;
+  }
+  throw Error(FTLM_ERR_ARG, "unsupported vectors per sweep: " + std::to_string(nv));
+}
+
+template <typename W>
+int64_t block_csr_device_t(Ctx& c, DBuf& row_ptr, DBuf& col, DBuf& val, DBuf& diag) {
+  const int64_t D = c.blk.dim;
+  CsrParams<W> P;
+  P.g = c.geom;
+  if constexpr (sizeof(W) == 4) P.v = view32(c);
+  else P.v = view64(c);
+  DBuf& cnt = c.sec.tmp_a;
+  cnt.ensure(sizeof(int32_t) * std::max<int64_t>(D, 1));
+  DBuf& rp64 = c.sec.tmp_d;
+  rp64.ensure(sizeof(int64_t) * (D + 1));
+  k_csr<W><<<grid_for(D, 128), 128, 0, c.stream>>>(P, c.binom.as<uint64_t>(), 0, cnt.as<int32_t>(), nullptr, nullptr,
+                                                    nullptr, nullptr);
+  FTLM_LAUNCH_CHECK();
+  const int64_t nnz = scan_excl_i32_to_i64(c, cnt.as<int32_t>(), rp64.as<int64_t>(), D);
+  FTLM_CUDA(cudaMemcpyAsync(rp64.as<int64_t>() + D, &nnz, sizeof(int64_t), cudaMemcpyHostToDevice, c.stream));
+  if (nnz > 0x7fffffffLL) throw Error(FTLM_ERR_CAPACITY, "block CSR exceeds 2^31 entries");
+  row_ptr.ensure(sizeof(int32_t) * (D + 1));
+  col.ensure(sizeof(int32_t) * std::max<int64_t>(nnz, 1));
+  val.ensure(sizeof(double) * 2 * std::max<int64_t>(nnz, 1));
+  diag.ensure(sizeof(double) * std::max<int64_t>(D, 1));
+  k_csr<W><<<grid_for(D, 128), 128, 0, c.stream>>>(P, c.binom.as<uint64_t>(), 1, nullptr, rp64.as<int64_t>(),
+                                                    col.as<int32_t>(), val.as<double>(), diag.as<double>());
+  k_i64_to_i32<<<grid_for(D + 1, 256), 256, 0, c.stream>>>(rp64.as<int64_t>(), row_ptr.as<int32_t>(), D + 1);
+  FTLM_LAUNCH_CHECK();
+  FTLM_CUDA(cudaStreamSynchronize(c.stream));
+  c.prof.kernel_launches += 3;
+  return nnz;
+}
+
+template <typename W>
+int64_t block_nonzero_hops_t(Ctx& c) {
+  const int64_t D = c.blk.dim;
+  if (D <= 0) return 0;
+  CsrParams<W> P;
+  P.g = c.geom;
+  if constexpr (sizeof(W) == 4) P.v = view32(c);
+  else P.v = view64(c);
+  DBuf& cnt = c.sec.tmp_a;
+  cnt.ensure(sizeof(int32_t) * D);
+  DBuf& rp64 = c.sec.tmp_d;
+  rp64.ensure(sizeof(int64_t) * (D + 1));
+  k_csr<W><<<grid_for(D, 128), 128, 0, c.stream>>>(P, c.binom.as<uint64_t>(), 2, cnt.as<int32_t>(), nullptr, nullptr,
+                                                    nullptr, nullptr);
+  FTLM_LAUNCH_CHECK();
+  return scan_excl_i32_to_i64(c, cnt.as<int32_t>(), rp64.as<int64_t>(), D);
+}
+
+}  // namespace
+
+int64_t block_nonzero_hops(Ctx& c) {
+  if (c.wide) return block_nonzero_hops_t<uint64_t>(c);
+  return block_nonzero_hops_t<uint32_t>(c);
+}
+
+int64_t block_csr_device(Ctx& c, DBuf& row_ptr, DBuf& col, DBuf& val, DBuf& diag) {
+  if (c.wide) return block_csr_device_t<uint64_t>(c, row_ptr, col, val, diag);
+  return block_csr_device_t<uint32_t>(c, row_ptr, col, val, diag);
+}
+
+void block_csr(Ctx& c, std::vector<int32_t>& row_ptr, std::vector<int32_t>& col, std::vector<double>& val,
+               std::vector<double>& diag) {
+  DBuf rp, cl, vl, dg;
+  const int64_t D = c.blk.dim;
+  const int64_t nnz = block_csr_device(c, rp, cl, vl, dg);
+  row_ptr.resize(D + 1);
+  col.resize(nnz);
+  val.resize(2 * nnz);
+  diag.resize(D);
+  FTLM_CUDA(cudaMemcpy(row_ptr.data(), rp.p, sizeof(int32_t) * (D + 1), cudaMemcpyDeviceToHost));
+  if (nnz) {
+    FTLM_CUDA(cudaMemcpy(col.data(), cl.p, sizeof(int32_t) * nnz, cudaMemcpyDeviceToHost));
+    FTLM_CUDA(cudaMemcpy(val.data(), vl.p, sizeof(double) * 2 * nnz, cudaMemcpyDeviceToHost));
+  }
+  if (D) FTLM_CUDA(cudaMemcpy(diag.data(), dg.p, sizeof(double) * D, cudaMemcpyDeviceToHost));
+  rp.release();
+  cl.release();
+  vl.release();
+  dg.release();
+}
+
+// Grid of the H*V kernel: one warp per row when the block is small, else
+// a whole number of waves over the SMs (CTAs resident per SM from the
+// occupancy calculator), rows handed out round-robin to warps.
+int hv_grid(Ctx& c, int nv, bool fp32) {
+  const int64_t by_rows = (c.blk.dim + kHvWarps - 1) / kHvWarps;
+  int per_sm = 1;
+  hv_apply(c, nullptr, &per_sm, nv, fp32, nullptr, nullptr, -1);
+  const int64_t cap = static_cast<int64_t>(c.sm_count) * per_sm;
+  return static_cast<int>(std::max<int64_t>(1, std::min(by_rows, cap)));
+}
+
+void hv_apply(Ctx& c, const void* in, void* out, int nv, bool fp32, const double* scale, double* partial,
+              int grid) {
+  if (grid == 0) grid = hv_grid(c, nv, fp32);
+  if (c.wide) {
+    if (fp32) launch_hv_nv<uint64_t, uint64_t, float>(c, in, out, nv, scale, partial, grid);
+    else launch_hv_nv<uint64_t, uint64_t, double>(c, in, out, nv, scale, partial, grid);
+  } else {
+    if (fp32) launch_hv_nv<uint32_t, uint32_t, float>(c, in, out, nv, scale, partial, grid);
+    else launch_hv_nv<uint32_t, uint32_t, double>(c, in, out, nv, scale, partial, grid);
+  }
+  if (grid < 0) return;
+  FTLM_LAUNCH_CHECK();
+  c.prof.kernel_launches += 1;
+}
+
+}  // namespace ftlm

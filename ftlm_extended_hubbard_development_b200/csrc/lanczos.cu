@@ -1,0 +1,574 @@
+// FTLM block: multi-vector Lanczos on the GPU (run_ftlm_block,
+// main.cpp:996-1113).
+//
+// All random vectors of a sweep advance together: one H*V launch per step
+// serves nv vectors. Per step
+//   hv        y = s_j H w_j (on the fly), partial Re<s_j w_j, y>
+//   alpha     alpha_j = sum of partials (fixed order, FP64)
+//   update    w_{j+1} = y - alpha_j s_j w_j - beta_{j-1} s_{j-1} w_{j-1},
+//             partial |w_{j+1}|^2 (FP64)
+//   beta      beta_j = sqrt(sum); s_{j+1} = 1/beta_j, or stop the vector
+//             at beta_j < 1e-12 / the last step (main.cpp:1044-1048)
+// Vectors stay unnormalised (q_j = s_j w_j) so no separate scaling pass is
+// needed. No re-orthogonalisation, as in the reference. The tridiagonal
+// matrices are then solved in one batched launch by implicit QL with
+// shifts, tracking only the first row of the eigenvector matrix
+// (Golub-Welsch), which gives the Ritz values and the FTLM weights v1^2/R.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <atomic>
+#include <random>
+#include <thread>
+
+#include "ftlm_internal.h"
+
+namespace ftlm {
+
+namespace {
+
+constexpr int kUpdThreads = 256;
+
+template <typename T>
+struct VT;
+template <>
+struct VT<float> {
+  using V = float4;
+  static constexpr int VPL = 2;
+};
+template <>
+struct VT<double> {
+  using V = double2;
+  static constexpr int VPL = 1;
+};
+
+// Lanczos state block (doubles), NV entries each.
+enum { S_CUR = 0, S_PREV = 1, S_BPREV = 2, S_CA = 3, S_CB = 4, S_DONE = 5, S_STEPS = 6, S_NFIELD = 7 };
+
+__global__ void k_state_init(double* st, int NV, int nva) {
+  const int v = threadIdx.x;
+  if (v >= NV) return;
+  st[S_CUR * NV + v] = v < nva ? 1.0 : 0.0;
+  st[S_PREV * NV + v] = 0.0;
+  st[S_BPREV * NV + v] = 0.0;
+  st[S_CA * NV + v] = 0.0;
+  st[S_CB * NV + v] = 0.0;
+  st[S_DONE * NV + v] = v < nva ? 0.0 : 1.0;
+  st[S_STEPS * NV + v] = v < nva ? 0.0 : 1.0;
+}
+
+__global__ void k_alpha_fin(int NV, int ncta, const double* __restrict__ partial, double* __restrict__ st,
+                            double* __restrict__ alpha_j) {
+  const int v = threadIdx.x;
+  if (v >= NV) return;
+  double s = 0.0;
+  for (int b = 0; b < ncta; ++b) s += partial[static_cast<int64_t>(b) * NV + v];
+  alpha_j[v] = s;
+  st[S_CA * NV + v] = s * st[S_CUR * NV + v];
+  st[S_CB * NV + v] = st[S_BPREV * NV + v] * st[S_PREV * NV + v];
+}
+
+__global__ void k_beta_fin(int NV, int ncta, const double* __restrict__ partial, double* __restrict__ st,
+                           double* __restrict__ beta_j, int j, int kdim) {
+  const int v = threadIdx.x;
+  if (v >= NV) return;
+  if (st[S_DONE * NV + v] != 0.0) {
+    st[S_CUR * NV + v] = 0.0;
+    st[S_PREV * NV + v] = 0.0;
+    st[S_BPREV * NV + v] = 0.0;
+    return;
+  }
+  double s = 0.0;
+  for (int b = 0; b < ncta; ++b) s += partial[static_cast<int64_t>(b) * NV + v];
+  const double bet = sqrt(s);
+  if (bet < 1e-12 || j + 1 == kdim) {
+    st[S_STEPS * NV + v] = static_cast<double>(j + 1);
+    st[S_DONE * NV + v] = 1.0;
+    st[S_CUR * NV + v] = 0.0;
+    st[S_PREV * NV + v] = 0.0;
+    st[S_BPREV * NV + v] = 0.0;
+    return;
+  }
+  beta_j[v] = bet;
+  st[S_PREV * NV + v] = st[S_CUR * NV + v];
+  st[S_CUR * NV + v] = 1.0 / bet;
+  st[S_BPREV * NV + v] = bet;
+}
+
+// w_prev <- y - ca*w_cur - cb*w_prev, per-vector |.|^2 partials.
+template <typename T>
+__global__ void __launch_bounds__(kUpdThreads) k_update(int64_t nchunks, int NV, const typename VT<T>::V* __restrict__ y,
+                                                        const typename VT<T>::V* __restrict__ wc,
+                                                        typename VT<T>::V* __restrict__ wp,
+                                                        const double* __restrict__ st, double* __restrict__ partial) {
+  using V = typename VT<T>::V;
+  constexpr int VPL = VT<T>::VPL;
+  const int CPR = NV / VPL;
+  __shared__ double red[kUpdThreads * 2];
+  const int tid = threadIdx.x;
+  const int cv = tid % CPR;  // stride is a multiple of CPR, so fixed per thread
+  double ca[VPL], cb[VPL], acc[VPL];
+#pragma unroll
+  for (int e = 0; e < VPL; ++e) {
+    ca[e] = st[S_CA * NV + cv * VPL + e];
+    cb[e] = st[S_CB * NV + cv * VPL + e];
+    acc[e] = 0.0;
+  }
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * kUpdThreads;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * kUpdThreads + tid; i < nchunks; i += stride) {
+    const V h = y[i], x = wc[i], p = wp[i];
+    V r;
+    if constexpr (VPL == 2) {
+      const double r0 = static_cast<double>(h.x) - ca[0] * x.x - cb[0] * p.x;
+      const double r1 = static_cast<double>(h.y) - ca[0] * x.y - cb[0] * p.y;
+      const double r2 = static_cast<double>(h.z) - ca[1] * x.z - cb[1] * p.z;
+      const double r3 = static_cast<double>(h.w) - ca[1] * x.w - cb[1] * p.w;
+      r = make_float4(static_cast<float>(r0), static_cast<float>(r1), static_cast<float>(r2), static_cast<float>(r3));
+      acc[0] += static_cast<double>(r.x) * r.x + static_cast<double>(r.y) * r.y;
+      acc[1] += static_cast<double>(r.z) * r.z + static_cast<double>(r.w) * r.w;
+    } else {
+      r.x = h.x - ca[0] * x.x - cb[0] * p.x;
+      r.y = h.y - ca[0] * x.y - cb[0] * p.y;
+      acc[0] += r.x * r.x + r.y * r.y;
+    }
+    wp[i] = r;
+  }
+#pragma unroll
+  for (int e = 0; e < VPL; ++e) red[tid * VPL + e] = acc[e];
+  __syncthreads();
+  for (int v = tid; v < NV; v += kUpdThreads) {
+    const int c = v / VPL, e = v % VPL;
+    double s = 0.0;
+    for (int t = c; t < kUpdThreads; t += CPR) s += red[t * VPL + e];
+    partial[static_cast<int64_t>(blockIdx.x) * NV + v] = s;
+  }
+}
+
+// Start vectors, production mode: uniform phase, |q_i|^2 = 1/dim.
+// Philox4x32-10 keyed by the block seed, counter (row, sample).
+template <typename T>
+__global__ void k_start_philox(int64_t dim, int NV, int nva, int sample0, uint64_t seed, typename VT<T>::V* __restrict__ out) {
+  using V = typename VT<T>::V;
+  constexpr int VPL = VT<T>::VPL;
+  const int CPR = NV / VPL;
+  const double amp = 1.0 / sqrt(static_cast<double>(dim));
+  const int64_t n = dim * CPR;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t row = i / CPR;
+    const int c = static_cast<int>(i % CPR);
+    double re[VPL], im[VPL];
+#pragma unroll
+    for (int e = 0; e < VPL; ++e) {
+      const int v = c * VPL + e;
+      re[e] = 0.0;
+      im[e] = 0.0;
+      if (v < nva) {
+        P4 ctr;
+        ctr.x[0] = static_cast<uint32_t>(row);
+        ctr.x[1] = static_cast<uint32_t>(static_cast<uint64_t>(row) >> 32);
+        ctr.x[2] = static_cast<uint32_t>(sample0 + v);
+        ctr.x[3] = 0x46544C4Du;
+        const P4 r = philox4x32_10(ctr, static_cast<uint32_t>(seed), static_cast<uint32_t>(seed >> 32));
+        const uint64_t bits53 = (static_cast<uint64_t>(r.x[0]) << 21) ^ (r.x[1] >> 11);
+        const double u = static_cast<double>(bits53 & ((1ULL << 53) - 1)) * (1.0 / 9007199254740992.0);
+        double sn, cs;
+        sincospi(2.0 * u, &sn, &cs);
+        re[e] = amp * cs;
+        im[e] = amp * sn;
+      }
+    }
+    V o;
+    if constexpr (VPL == 2) {
+      o = make_float4(static_cast<float>(re[0]), static_cast<float>(im[0]), static_cast<float>(re[1]),
+                      static_cast<float>(im[1]));
+    } else {
+      o = make_double2(re[0], im[0]);
+    }
+    out[i] = o;
+  }
+}
+
+// Start vectors given per sample ([nva][dim] complex FP64) into [dim][NV].
+template <typename T>
+__global__ void k_start_gather(int64_t dim, int NV, int nva, const double2* __restrict__ src,
+                               typename VT<T>::V* __restrict__ out) {
+  using V = typename VT<T>::V;
+  constexpr int VPL = VT<T>::VPL;
+  const int CPR = NV / VPL;
+  const int64_t n = dim * CPR;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t row = i / CPR;
+    const int c = static_cast<int>(i % CPR);
+    double2 z[VPL];
+#pragma unroll
+    for (int e = 0; e < VPL; ++e) {
+      const int v = c * VPL + e;
+      z[e] = v < nva ? src[static_cast<int64_t>(v) * dim + row] : make_double2(0.0, 0.0);
+    }
+    V o;
+    if constexpr (VPL == 2) {
+      o = make_float4(static_cast<float>(z[0].x), static_cast<float>(z[0].y), static_cast<float>(z[1].x),
+                      static_cast<float>(z[1].y));
+    } else {
+      o = z[0];
+    }
+    out[i] = o;
+  }
+}
+
+// Implicit QL with shifts on each Lanczos tridiagonal (one thread per
+// vector), tracking the first row z of the eigenvector matrix; then an
+// ascending sort. Writes eigenvalues and z^2 * inv_r into [nva][K] rows.
+__global__ void k_tridiag(int nva, int NV, int K, const double* __restrict__ alpha, const double* __restrict__ beta,
+                          const double* __restrict__ st, double* __restrict__ dout, double* __restrict__ zout,
+                          double* __restrict__ escr, double inv_r, int* __restrict__ status) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nva) return;
+  const int n = static_cast<int>(st[S_STEPS * NV + v]);
+  double* d = dout + static_cast<int64_t>(v) * K;
+  double* z = zout + static_cast<int64_t>(v) * K;
+  double* e = escr + static_cast<int64_t>(v) * K;
+  for (int i = 0; i < n; ++i) {
+    d[i] = alpha[static_cast<int64_t>(i) * NV + v];
+    e[i] = i + 1 < n ? beta[static_cast<int64_t>(i) * NV + v] : 0.0;
+    z[i] = i == 0 ? 1.0 : 0.0;
+  }
+  const double eps = 2.220446049250313e-16;
+  for (int l = 0; l < n; ++l) {
+    int iter = 0;
+    while (true) {
+      int m = l;
+      for (; m < n - 1; ++m) {
+        const double dd = fabs(d[m]) + fabs(d[m + 1]);
+        if (fabs(e[m]) <= eps * dd) break;
+      }
+      if (m == l) break;
+      if (++iter > 200) {
+        atomicExch(status, 1);
+        break;
+      }
+      double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
+      double r = hypot(g, 1.0);
+      g = d[m] - d[l] + e[l] / (g + copysign(r, g));
+      double s = 1.0, c = 1.0, p = 0.0;
+      int i = m - 1;
+      bool underflow = false;
+      for (; i >= l; --i) {
+        double f = s * e[i];
+        const double b = c * e[i];
+        r = hypot(f, g);
+        e[i + 1] = r;
+        if (r == 0.0) {
+          d[i + 1] -= p;
+          e[m] = 0.0;
+          underflow = true;
+          break;
+        }
+        s = f / r;
+        c = g / r;
+        g = d[i + 1] - p;
+        r = (d[i] - g) * s + 2.0 * c * b;
+        p = s * r;
+        d[i + 1] = g + p;
+        g = c * r - b;
+        f = z[i + 1];
+        z[i + 1] = s * z[i] + c * f;
+        z[i] = c * z[i] - s * f;
+      }
+      if (underflow) continue;
+      d[l] -= p;
+      e[l] = g;
+      e[m] = 0.0;
+    }
+  }
+  for (int i = 1; i < n; ++i) {  // insertion sort, ascending
+    const double dk = d[i], zk = z[i];
+    int j = i - 1;
+    while (j >= 0 && d[j] > dk) {
+      d[j + 1] = d[j];
+      z[j + 1] = z[j];
+      --j;
+    }
+    d[j + 1] = dk;
+    z[j + 1] = zk;
+  }
+  for (int i = 0; i < n; ++i) z[i] = z[i] * z[i] * inv_r;
+}
+
+// Concatenate the per-vector spectra sample by sample (main.cpp:1097-1110).
+__global__ void k_compact(int nva, int NV, int K, const double* __restrict__ st, const double* __restrict__ d,
+                          const double* __restrict__ w, double* __restrict__ ev_out, double* __restrict__ w_out,
+                          int64_t* __restrict__ total) {
+  __shared__ int off[129];
+  if (threadIdx.x == 0) {
+    int o = 0;
+    for (int v = 0; v < nva; ++v) {
+      off[v] = o;
+      o += static_cast<int>(st[S_STEPS * NV + v]);
+    }
+    off[nva] = o;
+    *total = o;
+  }
+  __syncthreads();
+  for (int v = 0; v < nva; ++v) {
+    const int n = off[v + 1] - off[v];
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      ev_out[off[v] + i] = d[static_cast<int64_t>(v) * K + i];
+      w_out[off[v] + i] = w[static_cast<int64_t>(v) * K + i];
+    }
+  }
+}
+
+// Algorithmic-byte model count: nonzero-amplitude hops with active
+// targets per block (the h_nz of the H*V roofline).
+int next_pow2(int x) {
+  int p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
+
+uint64_t mix_u64(uint64_t value) {  // main.cpp:514-519
+  value += 0x9e3779b97f4a7c15ULL;
+  value = (value ^ (value >> 30U)) * 0xbf58476d1ce4e5b9ULL;
+  value = (value ^ (value >> 27U)) * 0x94d049bb133111ebULL;
+  return value ^ (value >> 31U);
+}
+
+}  // namespace
+
+uint64_t block_seed(uint64_t seed, int n_up, int n_dn, int mx, int my) {  // main.cpp:521-533
+  uint64_t s = mix_u64(seed);
+  s ^= mix_u64(static_cast<uint64_t>(n_up + 1));
+  s ^= mix_u64(static_cast<uint64_t>(n_dn + 17));
+  s ^= mix_u64(static_cast<uint64_t>(mx + 257));
+  s ^= mix_u64(static_cast<uint64_t>(my + 65537));
+  return mix_u64(s);
+}
+
+// Reference start vectors (main.cpp:1015-1025): libstdc++ mt19937_64 and
+// normal_distribution; g++ evaluates Complex(normal(rng), normal(rng))
+// right to left, so each element is (second draw, first draw).
+void reference_start_vectors(uint64_t bseed, int sample0, int nva, int64_t dim, double* out) {
+  auto work = [&](int v) {
+    std::mt19937_64 rng(mix_u64(bseed ^ static_cast<uint64_t>(sample0 + v)));
+    std::normal_distribution<double> normal(0.0, 1.0);
+    double* q = out + 2 * static_cast<int64_t>(v) * dim;
+    double n2 = 0.0;
+    for (int64_t i = 0; i < dim; ++i) {
+      const double first = normal(rng);
+      const double second = normal(rng);
+      q[2 * i] = second;
+      q[2 * i + 1] = first;
+      n2 += second * second + first * first;
+    }
+    const double nrm = std::sqrt(n2);
+    for (int64_t i = 0; i < 2 * dim; ++i) q[i] /= nrm;
+  };
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  if (nva == 1 || dim < 4096 || hw == 1) {
+    for (int v = 0; v < nva; ++v) work(v);
+    return;
+  }
+  std::vector<std::thread> th;
+  std::atomic<int> next{0};
+  for (unsigned t = 0; t < std::min<unsigned>(hw, static_cast<unsigned>(nva)); ++t)
+    th.emplace_back([&] {
+      for (int v = next++; v < nva; v = next++) work(v);
+    });
+  for (auto& t : th) t.join();
+}
+
+int64_t spectra_alloc(Ctx& c, int64_t count) {
+  const int64_t need = c.spectra_used + count;
+  if (static_cast<size_t>(need) * sizeof(double) > c.spectra.cap) {
+    DBuf n;
+    n.ensure(sizeof(double) * std::max<int64_t>(need * 2, 1 << 16));
+    if (c.spectra_used > 0)
+      FTLM_CUDA(cudaMemcpyAsync(n.p, c.spectra.p, sizeof(double) * c.spectra_used, cudaMemcpyDeviceToDevice, c.stream));
+    FTLM_CUDA(cudaStreamSynchronize(c.stream));
+    c.spectra.release();
+    c.spectra = n;
+  }
+  const int64_t off = c.spectra_used;
+  c.spectra_used = need;
+  return off;
+}
+
+void spectra_reset(Ctx& c) {
+  c.spectra_used = 0;
+  c.spec.clear();
+}
+
+void run_ftlm_block(Ctx& c, int n_up, int n_dn, int mx, int my, Spectrum& out, const double* host_start,
+                    std::vector<double>* alpha_out, std::vector<double>* beta_out, std::vector<int32_t>* steps_out) {
+  block_prepare(c, mx, my);
+  const int64_t D = c.blk.dim;
+  if (D <= 0) throw Error(FTLM_ERR_ARG, "empty block");
+  const int R = c.opts.samples;
+  const int K = static_cast<int>(std::min<int64_t>(c.opts.lanczos_steps, D));
+  const bool fp32 = c.opts.precision == FTLM_PREC_MIXED;
+  int nvmax = c.opts.batch_vectors > 0 ? c.opts.batch_vectors : std::min(R, 128);
+  nvmax = std::min(nvmax, 128);
+  const uint64_t bseed = block_seed(c.opts.seed, n_up, n_dn, mx, my);
+  const int64_t off = spectra_alloc(c, 2 * static_cast<int64_t>(R) * K);
+  if (alpha_out) {
+    alpha_out->assign(static_cast<size_t>(R) * c.opts.lanczos_steps, 0.0);
+    beta_out->assign(static_cast<size_t>(R) * c.opts.lanczos_steps, 0.0);
+    steps_out->assign(R, 0);
+  }
+  const int esize = fp32 ? 8 : 16;
+  int64_t pos = 0;
+  std::vector<double> hstart;
+  for (int s0 = 0; s0 < R; s0 += nvmax) {
+    const int nva = std::min(nvmax, R - s0);
+    const int NV = next_pow2(std::max(nva, fp32 ? 2 : 1));
+    const size_t bytes = static_cast<size_t>(D) * NV * esize;
+    c.vec_a.ensure(bytes);
+    c.vec_b.ensure(bytes);
+    c.vec_h.ensure(bytes);
+    const int CPR = fp32 ? NV / 2 : NV;
+    const int64_t nchunks = D * CPR;
+    const int sgrid = static_cast<int>(std::min<int64_t>((nchunks + 255) / 256, static_cast<int64_t>(c.sm_count) * 16));
+    // start vectors into vec_a
+    if (host_start || c.opts.start_vector == FTLM_START_REF_GAUSSIAN) {
+      const double* src = nullptr;
+      if (host_start) {
+        src = host_start + 2 * static_cast<int64_t>(s0) * D;
+      } else {
+        hstart.resize(2 * static_cast<size_t>(nva) * D);
+        reference_start_vectors(bseed, s0, nva, D, hstart.data());
+        src = hstart.data();
+      }
+      c.host_start.ensure(sizeof(double) * 2 * static_cast<size_t>(nva) * D);
+      FTLM_CUDA(cudaMemcpyAsync(c.host_start.p, src, sizeof(double) * 2 * static_cast<size_t>(nva) * D,
+                                cudaMemcpyHostToDevice, c.stream));
+      c.prof.h2d_bytes += sizeof(double) * 2 * static_cast<int64_t>(nva) * D;
+      if (fp32)
+        k_start_gather<float><<<sgrid, 256, 0, c.stream>>>(D, NV, nva, c.host_start.as<double2>(), c.vec_a.as<float4>());
+      else
+        k_start_gather<double><<<sgrid, 256, 0, c.stream>>>(D, NV, nva, c.host_start.as<double2>(), c.vec_a.as<double2>());
+    } else {
+      if (fp32)
+        k_start_philox<float><<<sgrid, 256, 0, c.stream>>>(D, NV, nva, s0, bseed, c.vec_a.as<float4>());
+      else
+        k_start_philox<double><<<sgrid, 256, 0, c.stream>>>(D, NV, nva, s0, bseed, c.vec_a.as<double2>());
+    }
+    FTLM_LAUNCH_CHECK();
+    FTLM_CUDA(cudaMemsetAsync(c.vec_b.p, 0, bytes, c.stream));
+    const int hgrid = hv_grid(c, NV, fp32);
+    const int ugrid = std::max(1, std::min<int>(static_cast<int>((nchunks + kUpdThreads - 1) / kUpdThreads),
+                                                c.sm_count * 8));
+    c.partial.ensure(sizeof(double) * static_cast<size_t>(std::max(hgrid, ugrid)) * NV);
+    c.lz_state.ensure(sizeof(double) * S_NFIELD * NV);
+    c.lz_alpha.ensure(sizeof(double) * static_cast<size_t>(K) * NV);
+    c.lz_beta.ensure(sizeof(double) * static_cast<size_t>(K) * NV);
+    FTLM_CUDA(cudaMemsetAsync(c.lz_beta.p, 0, sizeof(double) * static_cast<size_t>(K) * NV, c.stream));
+    double* st = c.lz_state.as<double>();
+    k_state_init<<<1, 128, 0, c.stream>>>(st, NV, nva);
+    void* cur = c.vec_a.p;
+    void* prev = c.vec_b.p;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> evs;
+    for (int j = 0; j < K; ++j) {
+      cudaEvent_t e0 = nullptr, e1 = nullptr;
+      if (c.timing) {
+        FTLM_CUDA(cudaEventCreate(&e0));
+        FTLM_CUDA(cudaEventCreate(&e1));
+        FTLM_CUDA(cudaEventRecord(e0, c.stream));
+      }
+      hv_apply(c, cur, c.vec_h.p, NV, fp32, st + S_CUR * NV, c.partial.as<double>(), hgrid);
+      if (c.timing) {
+        FTLM_CUDA(cudaEventRecord(e1, c.stream));
+        evs.emplace_back(e0, e1);
+      }
+      k_alpha_fin<<<1, 128, 0, c.stream>>>(NV, hgrid, c.partial.as<double>(), st, c.lz_alpha.as<double>() + static_cast<int64_t>(j) * NV);
+      if (fp32)
+        k_update<float><<<ugrid, kUpdThreads, 0, c.stream>>>(nchunks, NV, c.vec_h.as<float4>(), static_cast<const float4*>(cur),
+                                                             static_cast<float4*>(prev), st, c.partial.as<double>());
+      else
+        k_update<double><<<ugrid, kUpdThreads, 0, c.stream>>>(nchunks, NV, c.vec_h.as<double2>(), static_cast<const double2*>(cur),
+                                                              static_cast<double2*>(prev), st, c.partial.as<double>());
+      k_beta_fin<<<1, 128, 0, c.stream>>>(NV, ugrid, c.partial.as<double>(), st, c.lz_beta.as<double>() + static_cast<int64_t>(j) * NV, j, K);
+      FTLM_LAUNCH_CHECK();
+      c.prof.kernel_launches += 3;
+      std::swap(cur, prev);
+    }
+    // Ritz values and weights
+    c.ritz_tmp.ensure(sizeof(double) * 3 * static_cast<size_t>(nva) * K + sizeof(int) * 4 + sizeof(int64_t) * 2);
+    double* dtmp = c.ritz_tmp.as<double>();
+    double* ztmp = dtmp + static_cast<size_t>(nva) * K;
+    double* etmp = ztmp + static_cast<size_t>(nva) * K;
+    int* status = reinterpret_cast<int*>(etmp + static_cast<size_t>(nva) * K);
+    int64_t* total = reinterpret_cast<int64_t*>(status + 2);
+    FTLM_CUDA(cudaMemsetAsync(status, 0, sizeof(int), c.stream));
+    cudaEvent_t ee0 = nullptr, ee1 = nullptr;
+    if (c.timing) {
+      FTLM_CUDA(cudaEventCreate(&ee0));
+      FTLM_CUDA(cudaEventCreate(&ee1));
+      FTLM_CUDA(cudaEventRecord(ee0, c.stream));
+    }
+    k_tridiag<<<(nva + 31) / 32, 32, 0, c.stream>>>(nva, NV, K, c.lz_alpha.as<double>(), c.lz_beta.as<double>(), st, dtmp,
+                                                   ztmp, etmp, 1.0 / R, status);
+    if (c.timing) FTLM_CUDA(cudaEventRecord(ee1, c.stream));
+    k_compact<<<1, 256, 0, c.stream>>>(nva, NV, K, st, dtmp, ztmp, c.spectra.as<double>() + off + pos,
+                                       c.spectra.as<double>() + off + static_cast<int64_t>(R) * K + pos, total);
+    FTLM_LAUNCH_CHECK();
+    c.prof.kernel_launches += 4;
+    int64_t cnt = 0;
+    int hstatus = 0;
+    FTLM_CUDA(cudaMemcpyAsync(&cnt, total, sizeof(int64_t), cudaMemcpyDeviceToHost, c.stream));
+    FTLM_CUDA(cudaMemcpyAsync(&hstatus, status, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    if (alpha_out) {
+      std::vector<double> a(static_cast<size_t>(K) * NV), b(static_cast<size_t>(K) * NV), s(S_NFIELD * NV);
+      FTLM_CUDA(cudaMemcpyAsync(a.data(), c.lz_alpha.p, sizeof(double) * a.size(), cudaMemcpyDeviceToHost, c.stream));
+      FTLM_CUDA(cudaMemcpyAsync(b.data(), c.lz_beta.p, sizeof(double) * b.size(), cudaMemcpyDeviceToHost, c.stream));
+      FTLM_CUDA(cudaMemcpyAsync(s.data(), st, sizeof(double) * s.size(), cudaMemcpyDeviceToHost, c.stream));
+      FTLM_CUDA(cudaStreamSynchronize(c.stream));
+      const int L = c.opts.lanczos_steps;
+      for (int v = 0; v < nva; ++v) {
+        const int n = static_cast<int>(s[S_STEPS * NV + v]);
+        (*steps_out)[s0 + v] = n;
+        for (int j = 0; j < n; ++j) (*alpha_out)[static_cast<size_t>(s0 + v) * L + j] = a[static_cast<size_t>(j) * NV + v];
+        for (int j = 0; j + 1 < n; ++j) (*beta_out)[static_cast<size_t>(s0 + v) * L + j] = b[static_cast<size_t>(j) * NV + v];
+      }
+    }
+    FTLM_CUDA(cudaStreamSynchronize(c.stream));
+    if (hstatus) throw Error(FTLM_ERR_NUMERIC, "tridiagonal QL did not converge");
+    if (c.timing) {
+      for (auto& pr : evs) {
+        float ms = 0.f;
+        FTLM_CUDA(cudaEventElapsedTime(&ms, pr.first, pr.second));
+        c.prof.hv_ms += ms;
+        c.prof.hv_launches += 1;
+        cudaEventDestroy(pr.first);
+        cudaEventDestroy(pr.second);
+      }
+      float ms = 0.f;
+      FTLM_CUDA(cudaEventElapsedTime(&ms, ee0, ee1));
+      c.prof.eig_ms += ms;
+      cudaEventDestroy(ee0);
+      cudaEventDestroy(ee1);
+    }
+    if (c.timing) {
+      // algorithmic bytes per H*V launch: D*[nv*s*(1 + h_nz) + nv*s + m],
+      // h_nz*D = nonzero-amplitude hops to active targets, m = 8 B per row
+      const double s = fp32 ? 8.0 : 16.0;
+      const double nzh = static_cast<double>(block_nonzero_hops(c));
+      const double per = static_cast<double>(D) * nva * s * 2.0 + nzh * nva * s + static_cast<double>(D) * 8.0;
+      c.prof.hv_bytes += per * static_cast<double>(K);
+    }
+    c.last_kdim = K;
+    c.last_nv = NV;
+    pos += cnt;
+  }
+  out.ev_off = off;
+  out.w_off = off + static_cast<int64_t>(R) * K;
+  out.count = pos;
+  out.exact = false;
+  out.prefactor = static_cast<double>(D);
+  out.particles = n_up + n_dn;
+  out.dim = D;
+}
+
+}  // namespace ftlm
