@@ -118,26 +118,29 @@ def ncu_traffic():
         return None
 
 
-def cpu_baseline(threads: int):
+def cpu_baseline(threads: int, sweeps: int = 2, skip: int = 0):
     """The reference's own apply_hamiltonian (oracle/_ref/ref_bench, compiled
     from the reference sources) on a bounded sample: same lattice and
-    couplings, the largest sector it builds in seconds, 16 vectors x 2 sweeps."""
+    couplings, the largest sector it builds in seconds (4x4 (4,4), ~15 s),
+    16 vectors per sweep; the first `skip` sweeps are warm-up."""
     exe = os.path.join(HERE, "oracle", "_ref", "ref_bench")
     if not os.path.exists(exe):
         return None
-    args = [exe, "hv", "4", "4", "0", "0", "16", "2", "--", "--lx", "4", "--ly", "4", "--u", "7",
-            "--threads", str(threads), "--max-sector-dim", "100000000"]
+    args = [exe, "hv", "4", "4", "0", "0", "16", str(sweeps + skip), "--", "--lx", "4", "--ly", "4",
+            "--u", "7", "--threads", str(threads), "--max-sector-dim", "100000000"]
     r = subprocess.run(args, capture_output=True, text=True, env={**os.environ, "OPENBLAS_NUM_THREADS": "1"})
     if r.returncode != 0:
         return None
     j = json.loads(r.stdout.strip().splitlines()[-1])
-    D, nz, nv, sw = j["dim"], j["nnz_nonzero"], j["nvec"], j["sweeps"]
+    D, nz, nv = j["dim"], j["nnz_nonzero"], j["nvec"]
+    per = j["sweep_seconds"][skip:]
     bytes_per_sweep = D * nv * 16 * 2 + nz * nv * 16 + D * 8
-    gbs = bytes_per_sweep * sw / j["seconds"] / 1e9
+    gbs = bytes_per_sweep * len(per) / sum(per) / 1e9
     return {"value": gbs, "unit": "GB/s", "cores": j["threads"], "kind": "reference",
+            "per_sweep_gbs": [bytes_per_sweep / s / 1e9 for s in per],
             "sample": (f"reference apply_hamiltonian (FP64 CSR SpMV, OpenMP over vectors) on 4x4 U=7 "
-                       f"sector (4,4) k=(0,0), dim {D}, {nv} vectors x {sw} sweeps, "
-                       f"{j['seconds']:.3f} s; sector (8,8) itself needs ~15 min/30 GB to build on the CPU")}
+                       f"sector (4,4) k=(0,0), dim {D}, {nv} vectors x {len(per)} timed sweeps "
+                       f"({sum(per):.3f} s); sector (8,8) itself needs ~15 min and ~30 GB to build on the CPU")}
 
 
 def run_reference(args):
@@ -145,15 +148,11 @@ def run_reference(args):
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    base = cpu_baseline(threads)
+    base = cpu_baseline(threads, sweeps=max(args.steps, 1), skip=args.warmup)
     if base is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_bench not built (make -C oracle ref)"}))
         return
-    vals = []
-    for _ in range(args.warmup + args.steps):
-        b = cpu_baseline(threads)
-        vals.append(b["value"])
-    v = statistics.median(vals[args.warmup:]) if len(vals) > args.warmup else base["value"]
+    v = base["value"]
     line = {"metric": METRIC, "value": v, "unit": "GB/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "c128", "data": "synthetic (model-defined Hilbert space, Gaussian vectors)",
@@ -273,6 +272,7 @@ def run_ours(args):
 
 
 def main():
+    global SECTOR, STEPS
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
@@ -281,7 +281,11 @@ def main():
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--batch", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--sector", default="8,8", help="N_up,N_down of the 4x4 sector (profiling cases)")
+    ap.add_argument("--lanczos-steps", type=int, default=STEPS)
     args = ap.parse_args()
+    SECTOR = tuple(int(x) for x in args.sector.split(","))
+    STEPS = args.lanczos_steps
     if args.impl == "reference":
         run_reference(args)
     else:

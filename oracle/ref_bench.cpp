@@ -46,6 +46,7 @@ int main(int argc, char** argv) {
     const int threads = requested_omp_threads(params);
     double seconds = 0.0;
     long nvec = 0, sweeps = 0;
+    std::vector<double> sweep_s;
     if (mode == "hv") {
       nvec = nums.at(4);
       sweeps = nums.at(5);
@@ -59,10 +60,12 @@ int main(int argc, char** argv) {
       }
       const auto t1 = clk::now();
       for (long s = 0; s < sweeps; ++s) {
+        const auto ts = clk::now();
 #if defined(_OPENMP)
 #pragma omp parallel for schedule(static) num_threads(threads)
 #endif
         for (long v = 0; v < nvec; ++v) apply_hamiltonian(block, in[v], out[v]);
+        sweep_s.push_back(std::chrono::duration<double>(clk::now() - ts).count());
       }
       seconds = std::chrono::duration<double>(clk::now() - t1).count();
     } else if (mode == "block") {
@@ -75,11 +78,15 @@ int main(int argc, char** argv) {
       std::cerr << "bad mode\n";
       return 2;
     }
+    std::string per = "[";
+    for (std::size_t i = 0; i < sweep_s.size(); ++i) per += (i ? ", " : "") + std::to_string(sweep_s[i]);
+    per += "]";
     std::printf(
         "{\"mode\": \"%s\", \"dim\": %zu, \"nnz\": %zu, \"nnz_nonzero\": %zu, \"full_dim\": %zu, "
-        "\"threads\": %d, \"nvec\": %ld, \"sweeps\": %ld, \"setup_s\": %.6f, \"seconds\": %.6f}\n",
+        "\"threads\": %d, \"nvec\": %ld, \"sweeps\": %ld, \"setup_s\": %.6f, \"seconds\": %.6f, "
+        "\"sweep_seconds\": %s}\n",
         mode.c_str(), block.basis_dim, block.col_idx.size(), nnz_nonzero, sector.full_dim, threads, nvec, sweeps,
-        setup, seconds);
+        setup, seconds, per.c_str());
     return 0;
   } catch (const std::exception& ex) {
     std::cerr << "Error: " << ex.what() << "\n";
