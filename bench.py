@@ -109,13 +109,18 @@ class ClockSampler:
 
 
 def ncu_traffic():
-    """DRAM bytes per H*V launch from the committed ncu summary, if any."""
-    p = os.path.join(HERE, "profiles", "hv_block88_traffic.json")
-    try:
-        with open(p) as f:
-            return float(json.load(f)["dram_bytes_per_launch"])
-    except Exception:
+    """DRAM bytes per H*V launch of the bench block, from the committed
+    one-pass ncu summary (profiles/k_hv_4x4_sector88_nv128_mixed_traffic.md)."""
+    if SECTOR != (8, 8) or STEPS <= 0:
         return None
+    p = os.path.join(HERE, "profiles", "k_hv_4x4_sector88_nv128_mixed_traffic.md")
+    try:
+        for line in open(p):
+            if line.startswith("dram_bytes_per_launch:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
 
 
 def cpu_baseline(threads: int, sweeps: int = 2, skip: int = 0):
