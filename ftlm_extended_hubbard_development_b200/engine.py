@@ -64,7 +64,7 @@ EXPORTS = [
     "ftlm_thermo_configure", "ftlm_thermo_accumulate_block", "ftlm_thermo_accumulate_host",
     "ftlm_thermo_read", "ftlm_block_apply", "ftlm_block_lanczos",
     "ftlm_debug_sector_parents", "ftlm_debug_sector_relations", "ftlm_debug_block_csr",
-    "ftlm_profile_enable", "ftlm_profile_read", "ftlm_profile_reset",
+    "ftlm_profile_enable", "ftlm_profile_read", "ftlm_profile_reset", "ftlm_ritz_noalloc",
 ]
 
 _lib = None
@@ -100,6 +100,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "ftlm_profile_enable": ([vp, i32], C.c_int),
         "ftlm_profile_read": ([vp, P(_Profile)], C.c_int),
         "ftlm_profile_reset": ([vp], C.c_int),
+        "ftlm_ritz_noalloc": ([vp, vp, vp, i32, i32, d, vp, vp, vp, vp, C.c_char_p, sz], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

@@ -165,6 +165,32 @@ int ftlm_debug_block_csr(ftlm_ctx* ctx, int32_t mx, int32_t my, double* diag, in
                          int32_t* col, double* val, size_t dim_cap, size_t nnz_cap,
                          size_t* dim, size_t* nnz);
 
+/* Allocation-free Ritz stage. No counterpart in the reference: it exists for
+ * callers that cannot allocate device memory when they need the Ritz values,
+ * e.g. a host framework whose caching allocator already holds the device's
+ * memory pool, or a latency-critical loop that cannot afford cudaMalloc /
+ * cudaFree (cudaFree synchronises the device). It computes what
+ * ftlm_block_spectrum returns for an FTLM block from Lanczos coefficients the
+ * caller holds on the device, without allocating anything.
+ *  - alpha, beta: device arrays [nvec][ld] (the layout ftlm_block_lanczos
+ *    returns on the host); steps: device [nvec], the alphas taken per vector.
+ *  - evals, weights: device outputs of at least nvec*ld doubles; each vector's
+ *    Ritz values ascending with weights v1^2 * inv_samples, concatenated vector
+ *    by vector. count (device, may be NULL) receives the total, or -1 when a
+ *    QL iteration failed to converge.
+ *  - Runs on `stream` (a cudaStream_t; NULL = default stream) of the current
+ *    device. Work space: a fixed device array of 3*FTLM_NOALLOC_MAX_ENTRIES
+ *    doubles (1.5 MiB) that every device loading the library keeps until the
+ *    process exits; nvec > 128 or nvec*ld > FTLM_NOALLOC_MAX_ENTRIES is
+ *    rejected with FTLM_ERR_CAPACITY. All calls share that array: calls that
+ *    overlap on the GPU race. The first call on a device looks up the array's
+ *    address; make it before any stream capture.
+ *  - errbuf (may be NULL) receives a message on failure. */
+#define FTLM_NOALLOC_MAX_ENTRIES 65536
+int ftlm_ritz_noalloc(const double* alpha, const double* beta, const int32_t* steps, int32_t nvec, int32_t ld,
+                      double inv_samples, double* evals, double* weights, int64_t* count, void* stream,
+                      char* errbuf, size_t errlen);
+
 /* Instrumentation: per-kernel CUDA-event timing (adds a sync per timed
  * launch), and the counters accumulated since the last reset. */
 int ftlm_profile_enable(ftlm_ctx* ctx, int32_t on);
