@@ -5,6 +5,7 @@
 // message for ftlm_last_error. No exception crosses the ABI.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -130,6 +131,7 @@ int ftlm_ctx_create(const ftlm_model* model, const ftlm_run_opts* opts, ftlm_ctx
   c.opts = *opts;
   c.device = opts->device;
   c.wide = model->lx * model->ly > 32;
+  if (const char* hv = std::getenv("FTLM_HV_VARIANT")) c.hv_forced = std::atoi(hv);
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0 || c.device < 0 || c.device >= ndev) {
     cudaGetLastError();
@@ -474,6 +476,8 @@ int ftlm_profile_read(ftlm_ctx* ctx, ftlm_profile* out) {
     out->kernel_launches = p.kernel_launches;
     out->h2d_bytes = p.h2d_bytes;
     out->d2h_bytes = p.d2h_bytes;
+    out->hv_variant = p.hv_variant;
+    out->tune_runs = p.tune_runs;
   });
 }
 

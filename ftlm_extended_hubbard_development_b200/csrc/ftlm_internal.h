@@ -136,6 +136,8 @@ struct Profile {
   double block_ms = 0.0;
   int64_t kernel_launches = 0;
   int64_t h2d_bytes = 0, d2h_bytes = 0;
+  int hv_variant = -1;  // H*V kernel variant of the last launch
+  int tune_runs = 0;    // autotuner measurements made by this context
 };
 
 struct Ctx {
@@ -143,6 +145,7 @@ struct Ctx {
   ftlm_run_opts opts{};
   Geom geom{};
   bool wide = false;  // 64-bit spin words (more than 32 sites)
+  int hv_forced = -1; // H*V kernel variant forced by FTLM_HV_VARIANT (-1: autotune)
   int device = 0;
   int sm_count = 148;
   cudaStream_t stream = nullptr;

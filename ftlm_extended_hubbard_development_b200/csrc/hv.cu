@@ -15,6 +15,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
 
 #include "ftlm_internal.h"
 
@@ -178,6 +181,22 @@ __device__ __forceinline__ int kth_bit(W x, int k) {
   return pos;
 }
 
+// Gathered vector rows stream through without allocating in L1, so the small
+// orbit tables of the target lookups (up_info, class tables, offsets) stay
+// L1-resident; L2 still caches the rows.
+__device__ __forceinline__ float4 ld_stream(const float4* p) {
+  float4 r;
+  asm("ld.global.nc.L1::no_allocate.v4.f32 {%0, %1, %2, %3}, [%4];"
+      : "=f"(r.x), "=f"(r.y), "=f"(r.z), "=f"(r.w)
+      : "l"(p));
+  return r;
+}
+__device__ __forceinline__ double2 ld_stream(const double2* p) {
+  double2 r;
+  asm("ld.global.nc.L1::no_allocate.v2.f64 {%0, %1}, [%2];" : "=d"(r.x), "=d"(r.y) : "l"(p));
+  return r;
+}
+
 template <typename T>
 __device__ __forceinline__ void cfma(typename CT<T>::V& acc, T cr, T ci, const typename CT<T>::V& x);
 
@@ -246,8 +265,10 @@ __device__ __forceinline__ double2 finish_row(const double2& x, const double2& a
 // chunks. scale[v] multiplies the result of vector v (Lanczos vectors are
 // stored unnormalised). partial[block][NV] receives Re<s*in, out> sums
 // (deterministic order), or nothing when partial == nullptr.
-template <typename W, typename R, typename T, int NV>
-__global__ void __launch_bounds__(kHvThreads) k_hv(const __grid_constant__ HvParams<W> P,
+// U: hops gathered per lane group per iteration (loads in flight);
+// MINB: CTAs per SM the register budget is sized for.
+template <typename W, typename R, typename T, int NV, int U, int MINB>
+__global__ void __launch_bounds__(kHvThreads, MINB) k_hv(const __grid_constant__ HvParams<W> P,
                                                    const typename CT<T>::V* __restrict__ in,
                                                    typename CT<T>::V* __restrict__ out,
                                                    const double* __restrict__ scale, double* __restrict__ partial,
@@ -370,19 +391,31 @@ __global__ void __launch_bounds__(kHvThreads) k_hv(const __grid_constant__ HvPar
         }
       }
       const int nb = min(32, total - b);
-      for (int j = 0; j < nb; j += HPAR) {
-        const int src = (j + grp) & 31;
-        const int64_t c = __shfl_sync(0xffffffffu, col, src);
-        const T r = __shfl_sync(0xffffffffu, cr, src);
-        const T i = __shfl_sync(0xffffffffu, ci, src);
-        if (j + grp < nb && c >= 0) {
-          const V* rowp = in + c * CPR;
+      for (int j = 0; j < nb; j += HPAR * U) {
+        // U hops per lane group: all their loads are issued before any FMA,
+        // keeping U*LPL 16-byte gathers in flight per lane
+        int64_t c[U];
+        T r[U], i[U];
+        V x[U][LPL];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const int q = j + u * HPAR + grp;
+          c[u] = __shfl_sync(0xffffffffu, col, q & 31);
+          r[u] = __shfl_sync(0xffffffffu, cr, q & 31);
+          i[u] = __shfl_sync(0xffffffffu, ci, q & 31);
+          if (q >= nb) c[u] = -1;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
 #pragma unroll
           for (int l = 0; l < LPL; ++l) {
-            const V x = __ldg(rowp + l * G + sub);
-            cfma<T>(acc[l], r, i, x);
+            if (c[u] >= 0) x[u][l] = ld_stream(in + c[u] * CPR + l * G + sub);
+            else vzero(x[u][l]);
           }
-        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+#pragma unroll
+          for (int l = 0; l < LPL; ++l) cfma<T>(acc[l], r[u], i[u], x[u][l]);
       }
     }
     __syncwarp();
@@ -396,7 +429,7 @@ __global__ void __launch_bounds__(kHvThreads) k_hv(const __grid_constant__ HvPar
       const double diag = diag_energy(u, d, g);
 #pragma unroll
       for (int l = 0; l < LPL; ++l) {
-        const V x = __ldg(in + row * CPR + l * G + sub);
+        const V x = ld_stream(in + row * CPR + l * G + sub);
         out[row * CPR + l * G + sub] = finish_row(x, acc[l], diag, sc[l], dot[l]);
       }
     }
@@ -418,43 +451,81 @@ __global__ void __launch_bounds__(kHvThreads) k_hv(const __grid_constant__ HvPar
   }
 }
 
-template <typename W, typename R, typename T, int NV>
+template <typename W, typename R, typename T, int NV, int U, int MINB>
 void launch_hv_t(Ctx& c, const void* in, void* out, const double* scale, double* partial, int grid) {
-  if (grid < 0) {  // occupancy query: CTAs resident per SM
-    static int occ = 0;
-    if (!occ) {
-      FTLM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_hv<W, R, T, NV>, kHvThreads, 0));
-      occ = std::max(occ, 1);
-    }
-    *static_cast<int*>(out) = occ;
-    return;
-  }
   HvParams<W> P;
   P.g = c.geom;
   if constexpr (sizeof(W) == 4) P.v = view32(c);
   else P.v = view64(c);
   using V = typename CT<T>::V;
   const R* gb = sizeof(R) == 4 ? reinterpret_cast<const R*>(c.binom32.p) : reinterpret_cast<const R*>(c.binom.p);
-  k_hv<W, R, T, NV><<<grid, kHvThreads, 0, c.stream>>>(P, static_cast<const V*>(in), static_cast<V*>(out), scale,
-                                                       partial, gb);
+  k_hv<W, R, T, NV, U, MINB><<<grid, kHvThreads, 0, c.stream>>>(P, static_cast<const V*>(in), static_cast<V*>(out),
+                                                                scale, partial, gb);
+}
+
+// Kernel variants the autotuner chooses from: (gather unroll U, CTAs/SM).
+constexpr int kNumVariants = 5;
+constexpr int kVarU[kNumVariants] = {1, 2, 4, 4, 8};
+constexpr int kVarB[kNumVariants] = {4, 4, 3, 2, 2};
+
+template <typename W, typename R, typename T, int NV>
+void launch_hv_var(Ctx& c, int var, const void* in, void* out, const double* scale, double* partial, int grid) {
+  switch (var) {
+    case 0: launch_hv_t<W, R, T, NV, 1, 4>(c, in, out, scale, partial, grid); return;
+    case 1: launch_hv_t<W, R, T, NV, 2, 4>(c, in, out, scale, partial, grid); return;
+    case 2: launch_hv_t<W, R, T, NV, 4, 3>(c, in, out, scale, partial, grid); return;
+    case 3: launch_hv_t<W, R, T, NV, 4, 2>(c, in, out, scale, partial, grid); return;
+    case 4: launch_hv_t<W, R, T, NV, 8, 2>(c, in, out, scale, partial, grid); return;
+    default: break;
+  }
+  throw Error(FTLM_ERR_ARG, "bad H*V kernel variant");
 }
 
 template <typename W, typename R, typename T>
-void launch_hv_nv(Ctx& c, const void* in, void* out, int nv, const double* scale, double* partial, int grid) {
+void launch_hv_nv(Ctx& c, int var, const void* in, void* out, int nv, const double* scale, double* partial,
+                  int grid) {
   switch (nv) {
     case 1:
-      if constexpr (sizeof(T) == 8) { launch_hv_t<W, R, T, 1>(c, in, out, scale, partial, grid); return; }
+      if constexpr (sizeof(T) == 8) { launch_hv_var<W, R, T, 1>(c, var, in, out, scale, partial, grid); return; }
       break;
-    case 2: launch_hv_t<W, R, T, 2>(c, in, out, scale, partial, grid); return;
-    case 4: launch_hv_t<W, R, T, 4>(c, in, out, scale, partial, grid); return;
-    case 8: launch_hv_t<W, R, T, 8>(c, in, out, scale, partial, grid); return;
-    case 16: launch_hv_t<W, R, T, 16>(c, in, out, scale, partial, grid); return;
-    case 32: launch_hv_t<W, R, T, 32>(c, in, out, scale, partial, grid); return;
-    case 64: launch_hv_t<W, R, T, 64>(c, in, out, scale, partial, grid); return;
-    case 128: launch_hv_t<W, R, T, 128>(c, in, out, scale, partial, grid); return;
+    case 2: launch_hv_var<W, R, T, 2>(c, var, in, out, scale, partial, grid); return;
+    case 4: launch_hv_var<W, R, T, 4>(c, var, in, out, scale, partial, grid); return;
+    case 8: launch_hv_var<W, R, T, 8>(c, var, in, out, scale, partial, grid); return;
+    case 16: launch_hv_var<W, R, T, 16>(c, var, in, out, scale, partial, grid); return;
+    case 32: launch_hv_var<W, R, T, 32>(c, var, in, out, scale, partial, grid); return;
+    case 64: launch_hv_var<W, R, T, 64>(c, var, in, out, scale, partial, grid); return;
+    case 128: launch_hv_var<W, R, T, 128>(c, var, in, out, scale, partial, grid); return;
     default: break;
   }
   throw Error(FTLM_ERR_ARG, "unsupported vectors per sweep: " + std::to_string(nv));
+}
+
+void launch_any(Ctx& c, int var, const void* in, void* out, int nv, bool fp32, const double* scale,
+                double* partial, int grid) {
+  if (c.wide) {
+    if (fp32) launch_hv_nv<uint64_t, uint64_t, float>(c, var, in, out, nv, scale, partial, grid);
+    else launch_hv_nv<uint64_t, uint64_t, double>(c, var, in, out, nv, scale, partial, grid);
+  } else {
+    if (fp32) launch_hv_nv<uint32_t, uint32_t, float>(c, var, in, out, nv, scale, partial, grid);
+    else launch_hv_nv<uint32_t, uint32_t, double>(c, var, in, out, nv, scale, partial, grid);
+  }
+}
+
+// Autotuner: the first time an H*V of a given (word size, precision, vectors
+// per sweep, block-size class) runs on a block big enough to measure, every
+// variant is timed on that block (output to the caller's scratch, no state
+// touched) and the fastest is kept for the process. Results do not depend on
+// the variant (same grid, same summation order).
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int, int>, int> g_tuned;
+
+int size_class(int64_t dim) {
+  int k = 0;
+  while (dim >= 16 && k < 40) {
+    dim >>= 2;
+    ++k;
+  }
+  return k;
 }
 
 template <typename W>
@@ -541,25 +612,65 @@ void block_csr(Ctx& c, std::vector<int32_t>& row_ptr, std::vector<int32_t>& col,
 // Grid of the H*V kernel: one warp per row when the block is small, else
 // a whole number of waves over the SMs (CTAs resident per SM from the
 // occupancy calculator), rows handed out round-robin to warps.
+// Grid of the H*V kernel: one warp per row for small blocks, else four CTAs
+// per SM (rows round-robin over warps). Independent of the kernel variant, so
+// the order of the per-CTA dot-product partials is too.
 int hv_grid(Ctx& c, int nv, bool fp32) {
+  (void)nv;
+  (void)fp32;
   const int64_t by_rows = (c.blk.dim + kHvWarps - 1) / kHvWarps;
-  int per_sm = 1;
-  hv_apply(c, nullptr, &per_sm, nv, fp32, nullptr, nullptr, -1);
-  const int64_t cap = static_cast<int64_t>(c.sm_count) * per_sm;
+  const int64_t cap = static_cast<int64_t>(c.sm_count) * 4;
   return static_cast<int>(std::max<int64_t>(1, std::min(by_rows, cap)));
+}
+
+int hv_variant(Ctx& c, const void* in, void* out, int nv, bool fp32, int grid) {
+  if (c.hv_forced >= 0 && c.hv_forced < kNumVariants) return c.hv_forced;
+  const auto key = std::make_tuple(c.wide ? 1 : 0, fp32 ? 1 : 0, nv, size_class(c.blk.dim), c.device);
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tuned.find(key);
+    if (it != g_tuned.end()) return it->second;
+  }
+  if (c.blk.dim < (1 << 15)) return 1;  // too small to measure; launch overhead dominates
+  cudaEvent_t e0, e1;
+  FTLM_CUDA(cudaEventCreate(&e0));
+  FTLM_CUDA(cudaEventCreate(&e1));
+  // best of 3 single-launch timings per variant, variants interleaved so a
+  // clock or power transient does not favour one of them
+  float best_ms[kNumVariants];
+  for (int v = 0; v < kNumVariants; ++v) {
+    best_ms[v] = 1e30f;
+    launch_any(c, v, in, out, nv, fp32, nullptr, nullptr, grid);  // warm
+  }
+  for (int rep = 0; rep < 3; ++rep)
+    for (int v = 0; v < kNumVariants; ++v) {
+      FTLM_CUDA(cudaEventRecord(e0, c.stream));
+      launch_any(c, v, in, out, nv, fp32, nullptr, nullptr, grid);
+      FTLM_CUDA(cudaEventRecord(e1, c.stream));
+      FTLM_LAUNCH_CHECK();
+      FTLM_CUDA(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      FTLM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      best_ms[v] = std::min(best_ms[v], ms);
+    }
+  int best = 0;
+  for (int v = 1; v < kNumVariants; ++v)
+    if (best_ms[v] < best_ms[best]) best = v;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c.prof.tune_runs += 1;
+  c.prof.kernel_launches += 4 * kNumVariants;
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  g_tuned[key] = best;
+  return best;
 }
 
 void hv_apply(Ctx& c, const void* in, void* out, int nv, bool fp32, const double* scale, double* partial,
               int grid) {
   if (grid == 0) grid = hv_grid(c, nv, fp32);
-  if (c.wide) {
-    if (fp32) launch_hv_nv<uint64_t, uint64_t, float>(c, in, out, nv, scale, partial, grid);
-    else launch_hv_nv<uint64_t, uint64_t, double>(c, in, out, nv, scale, partial, grid);
-  } else {
-    if (fp32) launch_hv_nv<uint32_t, uint32_t, float>(c, in, out, nv, scale, partial, grid);
-    else launch_hv_nv<uint32_t, uint32_t, double>(c, in, out, nv, scale, partial, grid);
-  }
-  if (grid < 0) return;
+  const int var = hv_variant(c, in, out, nv, fp32, grid);
+  c.prof.hv_variant = var;
+  launch_any(c, var, in, out, nv, fp32, scale, partial, grid);
   FTLM_LAUNCH_CHECK();
   c.prof.kernel_launches += 1;
 }

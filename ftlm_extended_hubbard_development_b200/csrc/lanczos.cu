@@ -218,21 +218,44 @@ __global__ void k_start_gather(int64_t dim, int NV, int nva, const double2* __re
   }
 }
 
-// Implicit QL with shifts on each Lanczos tridiagonal (one thread per
-// vector), tracking the first row z of the eigenvector matrix; then an
-// ascending sort. Writes eigenvalues and z^2 * inv_r into [nva][K] rows.
-__global__ void k_tridiag(int nva, int NV, int K, const double* __restrict__ alpha, const double* __restrict__ beta,
-                          const double* __restrict__ st, double* __restrict__ dout, double* __restrict__ zout,
-                          double* __restrict__ escr, double inv_r, int* __restrict__ status) {
-  const int v = blockIdx.x * blockDim.x + threadIdx.x;
-  if (v >= nva) return;
-  const int n = static_cast<int>(st[S_STEPS * NV + v]);
-  double* d = dout + static_cast<int64_t>(v) * K;
-  double* z = zout + static_cast<int64_t>(v) * K;
-  double* e = escr + static_cast<int64_t>(v) * K;
+// Strided view of one vector's work array (shared memory: stride 32, one
+// column per thread; global memory: stride 1, one row per thread).
+struct Col {
+  double* p;
+  int st;
+  __device__ __forceinline__ double& operator[](int i) const { return p[i * st]; }
+};
+
+// Implicit QL with shifts on every Lanczos tridiagonal of a block (one
+// thread per random vector, all sweeps of the block in one launch), tracking
+// the first row z of the eigenvector matrix; then an ascending sort.
+// alpha/beta are [sweep][K][ld] (vector r = sweep r/nvmax, lane r%nvmax),
+// steps[r] the alphas taken. Outputs eigenvalues and z^2 * inv_r into [R][K]
+// rows. With smem != 0 the three work columns of the warp's 32 vectors live
+// in shared memory ([3][K][32]), otherwise in global memory.
+__global__ void k_tridiag(int R, int nvmax, int ld, int K, const double* __restrict__ alpha,
+                          const double* __restrict__ beta, const int32_t* __restrict__ steps,
+                          double* __restrict__ dout, double* __restrict__ zout, double* __restrict__ escr,
+                          double inv_r, int* __restrict__ status, int smem) {
+  extern __shared__ double sm[];
+  const int t = threadIdx.x;
+  const int r = blockIdx.x * blockDim.x + t;
+  if (r >= R) return;
+  const int n = steps[r];
+  const int64_t base = (static_cast<int64_t>(r / nvmax) * K) * ld + r % nvmax;
+  Col d, z, e;
+  if (smem) {
+    d = {sm + t, 32};
+    z = {sm + 32 * K + t, 32};
+    e = {sm + 64 * K + t, 32};
+  } else {
+    d = {dout + static_cast<int64_t>(r) * K, 1};
+    z = {zout + static_cast<int64_t>(r) * K, 1};
+    e = {escr + static_cast<int64_t>(r) * K, 1};
+  }
   for (int i = 0; i < n; ++i) {
-    d[i] = alpha[static_cast<int64_t>(i) * NV + v];
-    e[i] = i + 1 < n ? beta[static_cast<int64_t>(i) * NV + v] : 0.0;
+    d[i] = alpha[base + static_cast<int64_t>(i) * ld];
+    e[i] = i + 1 < n ? beta[base + static_cast<int64_t>(i) * ld] : 0.0;
     z[i] = i == 0 ? 1.0 : 0.0;
   }
   const double eps = 2.220446049250313e-16;
@@ -250,29 +273,28 @@ __global__ void k_tridiag(int nva, int NV, int K, const double* __restrict__ alp
         break;
       }
       double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
-      double r = hypot(g, 1.0);
-      g = d[m] - d[l] + e[l] / (g + copysign(r, g));
+      double rr = hypot(g, 1.0);
+      g = d[m] - d[l] + e[l] / (g + copysign(rr, g));
       double s = 1.0, c = 1.0, p = 0.0;
-      int i = m - 1;
       bool underflow = false;
-      for (; i >= l; --i) {
+      for (int i = m - 1; i >= l; --i) {
         double f = s * e[i];
         const double b = c * e[i];
-        r = hypot(f, g);
-        e[i + 1] = r;
-        if (r == 0.0) {
+        rr = hypot(f, g);
+        e[i + 1] = rr;
+        if (rr == 0.0) {
           d[i + 1] -= p;
           e[m] = 0.0;
           underflow = true;
           break;
         }
-        s = f / r;
-        c = g / r;
+        s = f / rr;
+        c = g / rr;
         g = d[i + 1] - p;
-        r = (d[i] - g) * s + 2.0 * c * b;
-        p = s * r;
+        rr = (d[i] - g) * s + 2.0 * c * b;
+        p = s * rr;
         d[i + 1] = g + p;
-        g = c * r - b;
+        g = c * rr - b;
         f = z[i + 1];
         z[i + 1] = s * z[i] + c * f;
         z[i] = c * z[i] - s * f;
@@ -294,31 +316,44 @@ __global__ void k_tridiag(int nva, int NV, int K, const double* __restrict__ alp
     d[j + 1] = dk;
     z[j + 1] = zk;
   }
-  for (int i = 0; i < n; ++i) z[i] = z[i] * z[i] * inv_r;
+  double* dr = dout + static_cast<int64_t>(r) * K;
+  double* zr = zout + static_cast<int64_t>(r) * K;
+  for (int i = 0; i < n; ++i) {
+    const double zi = z[i];
+    dr[i] = d[i];
+    zr[i] = zi * zi * inv_r;
+  }
 }
 
 // Concatenate the per-vector spectra sample by sample (main.cpp:1097-1110).
-__global__ void k_compact(int nva, int NV, int K, const double* __restrict__ st, const double* __restrict__ d,
+// Dynamic shared memory: R+1 offsets.
+__global__ void k_compact(int R, int K, const int32_t* __restrict__ steps, const double* __restrict__ d,
                           const double* __restrict__ w, double* __restrict__ ev_out, double* __restrict__ w_out,
                           int64_t* __restrict__ total) {
-  __shared__ int off[129];
+  extern __shared__ int off[];
   if (threadIdx.x == 0) {
     int o = 0;
-    for (int v = 0; v < nva; ++v) {
+    for (int v = 0; v < R; ++v) {
       off[v] = o;
-      o += static_cast<int>(st[S_STEPS * NV + v]);
+      o += steps[v];
     }
-    off[nva] = o;
+    off[R] = o;
     *total = o;
   }
   __syncthreads();
-  for (int v = 0; v < nva; ++v) {
+  for (int v = 0; v < R; ++v) {
     const int n = off[v + 1] - off[v];
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
       ev_out[off[v] + i] = d[static_cast<int64_t>(v) * K + i];
       w_out[off[v] + i] = w[static_cast<int64_t>(v) * K + i];
     }
   }
+}
+
+// Steps of the nva vectors of one sweep, into the block's [R] array.
+__global__ void k_collect_steps(const double* __restrict__ st, int NV, int nva, int32_t* __restrict__ out) {
+  const int v = threadIdx.x;
+  if (v < nva) out[v] = static_cast<int32_t>(st[S_STEPS * NV + v]);
 }
 
 // Algorithmic-byte model count: nonzero-amplitude hops with active
@@ -419,8 +454,23 @@ void run_ftlm_block(Ctx& c, int n_up, int n_dn, int mx, int my, Spectrum& out, c
     steps_out->assign(R, 0);
   }
   const int esize = fp32 ? 8 : 16;
-  int64_t pos = 0;
+  const int nsweep = (R + nvmax - 1) / nvmax;
+  const int ld = next_pow2(std::max(nvmax, fp32 ? 2 : 1));  // alpha/beta row stride
+  c.lz_alpha.ensure(sizeof(double) * static_cast<size_t>(nsweep) * K * ld);
+  c.lz_beta.ensure(sizeof(double) * static_cast<size_t>(nsweep) * K * ld);
+  FTLM_CUDA(cudaMemsetAsync(c.lz_beta.p, 0, sizeof(double) * static_cast<size_t>(nsweep) * K * ld, c.stream));
+  c.ritz_tmp.ensure(sizeof(double) * 3 * static_cast<size_t>(R) * K + sizeof(int32_t) * (R + 8) + 64);
+  double* dtmp = c.ritz_tmp.as<double>();
+  double* ztmp = dtmp + static_cast<size_t>(R) * K;
+  double* etmp = ztmp + static_cast<size_t>(R) * K;
+  int32_t* steps_all = reinterpret_cast<int32_t*>(etmp + static_cast<size_t>(R) * K);
+  int* status = steps_all + R;
+  int64_t* total = reinterpret_cast<int64_t*>(reinterpret_cast<uintptr_t>(status + 2 + 7) & ~uintptr_t(7));
+  FTLM_CUDA(cudaMemsetAsync(status, 0, sizeof(int), c.stream));
   std::vector<double> hstart;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> evs;
+  double hv_bytes = 0.0;
+  const double nzh = c.timing ? static_cast<double>(block_nonzero_hops(c)) : 0.0;
   for (int s0 = 0; s0 < R; s0 += nvmax) {
     const int nva = std::min(nvmax, R - s0);
     const int NV = next_pow2(std::max(nva, fp32 ? 2 : 1));
@@ -462,14 +512,12 @@ void run_ftlm_block(Ctx& c, int n_up, int n_dn, int mx, int my, Spectrum& out, c
                                                 c.sm_count * 8));
     c.partial.ensure(sizeof(double) * static_cast<size_t>(std::max(hgrid, ugrid)) * NV);
     c.lz_state.ensure(sizeof(double) * S_NFIELD * NV);
-    c.lz_alpha.ensure(sizeof(double) * static_cast<size_t>(K) * NV);
-    c.lz_beta.ensure(sizeof(double) * static_cast<size_t>(K) * NV);
-    FTLM_CUDA(cudaMemsetAsync(c.lz_beta.p, 0, sizeof(double) * static_cast<size_t>(K) * NV, c.stream));
     double* st = c.lz_state.as<double>();
+    double* alpha = c.lz_alpha.as<double>() + static_cast<int64_t>(s0 / nvmax) * K * ld;
+    double* beta = c.lz_beta.as<double>() + static_cast<int64_t>(s0 / nvmax) * K * ld;
     k_state_init<<<1, 128, 0, c.stream>>>(st, NV, nva);
     void* cur = c.vec_a.p;
     void* prev = c.vec_b.p;
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> evs;
     for (int j = 0; j < K; ++j) {
       cudaEvent_t e0 = nullptr, e1 = nullptr;
       if (c.timing) {
@@ -482,89 +530,91 @@ void run_ftlm_block(Ctx& c, int n_up, int n_dn, int mx, int my, Spectrum& out, c
         FTLM_CUDA(cudaEventRecord(e1, c.stream));
         evs.emplace_back(e0, e1);
       }
-      k_alpha_fin<<<1, 128, 0, c.stream>>>(NV, hgrid, c.partial.as<double>(), st, c.lz_alpha.as<double>() + static_cast<int64_t>(j) * NV);
+      k_alpha_fin<<<1, 128, 0, c.stream>>>(NV, hgrid, c.partial.as<double>(), st, alpha + static_cast<int64_t>(j) * ld);
       if (fp32)
         k_update<float><<<ugrid, kUpdThreads, 0, c.stream>>>(nchunks, NV, c.vec_h.as<float4>(), static_cast<const float4*>(cur),
                                                              static_cast<float4*>(prev), st, c.partial.as<double>());
       else
         k_update<double><<<ugrid, kUpdThreads, 0, c.stream>>>(nchunks, NV, c.vec_h.as<double2>(), static_cast<const double2*>(cur),
                                                               static_cast<double2*>(prev), st, c.partial.as<double>());
-      k_beta_fin<<<1, 128, 0, c.stream>>>(NV, ugrid, c.partial.as<double>(), st, c.lz_beta.as<double>() + static_cast<int64_t>(j) * NV, j, K);
+      k_beta_fin<<<1, 128, 0, c.stream>>>(NV, ugrid, c.partial.as<double>(), st, beta + static_cast<int64_t>(j) * ld, j, K);
       FTLM_LAUNCH_CHECK();
       c.prof.kernel_launches += 3;
       std::swap(cur, prev);
     }
-    // Ritz values and weights
-    c.ritz_tmp.ensure(sizeof(double) * 3 * static_cast<size_t>(nva) * K + sizeof(int) * 4 + sizeof(int64_t) * 2);
-    double* dtmp = c.ritz_tmp.as<double>();
-    double* ztmp = dtmp + static_cast<size_t>(nva) * K;
-    double* etmp = ztmp + static_cast<size_t>(nva) * K;
-    int* status = reinterpret_cast<int*>(etmp + static_cast<size_t>(nva) * K);
-    int64_t* total = reinterpret_cast<int64_t*>(status + 2);
-    FTLM_CUDA(cudaMemsetAsync(status, 0, sizeof(int), c.stream));
-    cudaEvent_t ee0 = nullptr, ee1 = nullptr;
-    if (c.timing) {
-      FTLM_CUDA(cudaEventCreate(&ee0));
-      FTLM_CUDA(cudaEventCreate(&ee1));
-      FTLM_CUDA(cudaEventRecord(ee0, c.stream));
-    }
-    k_tridiag<<<(nva + 31) / 32, 32, 0, c.stream>>>(nva, NV, K, c.lz_alpha.as<double>(), c.lz_beta.as<double>(), st, dtmp,
-                                                   ztmp, etmp, 1.0 / R, status);
-    if (c.timing) FTLM_CUDA(cudaEventRecord(ee1, c.stream));
-    k_compact<<<1, 256, 0, c.stream>>>(nva, NV, K, st, dtmp, ztmp, c.spectra.as<double>() + off + pos,
-                                       c.spectra.as<double>() + off + static_cast<int64_t>(R) * K + pos, total);
+    k_collect_steps<<<1, 128, 0, c.stream>>>(st, NV, nva, steps_all + s0);
     FTLM_LAUNCH_CHECK();
-    c.prof.kernel_launches += 4;
-    int64_t cnt = 0;
-    int hstatus = 0;
-    FTLM_CUDA(cudaMemcpyAsync(&cnt, total, sizeof(int64_t), cudaMemcpyDeviceToHost, c.stream));
-    FTLM_CUDA(cudaMemcpyAsync(&hstatus, status, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
-    if (alpha_out) {
-      std::vector<double> a(static_cast<size_t>(K) * NV), b(static_cast<size_t>(K) * NV), s(S_NFIELD * NV);
-      FTLM_CUDA(cudaMemcpyAsync(a.data(), c.lz_alpha.p, sizeof(double) * a.size(), cudaMemcpyDeviceToHost, c.stream));
-      FTLM_CUDA(cudaMemcpyAsync(b.data(), c.lz_beta.p, sizeof(double) * b.size(), cudaMemcpyDeviceToHost, c.stream));
-      FTLM_CUDA(cudaMemcpyAsync(s.data(), st, sizeof(double) * s.size(), cudaMemcpyDeviceToHost, c.stream));
-      FTLM_CUDA(cudaStreamSynchronize(c.stream));
-      const int L = c.opts.lanczos_steps;
-      for (int v = 0; v < nva; ++v) {
-        const int n = static_cast<int>(s[S_STEPS * NV + v]);
-        (*steps_out)[s0 + v] = n;
-        for (int j = 0; j < n; ++j) (*alpha_out)[static_cast<size_t>(s0 + v) * L + j] = a[static_cast<size_t>(j) * NV + v];
-        for (int j = 0; j + 1 < n; ++j) (*beta_out)[static_cast<size_t>(s0 + v) * L + j] = b[static_cast<size_t>(j) * NV + v];
-      }
-    }
-    FTLM_CUDA(cudaStreamSynchronize(c.stream));
-    if (hstatus) throw Error(FTLM_ERR_NUMERIC, "tridiagonal QL did not converge");
-    if (c.timing) {
-      for (auto& pr : evs) {
-        float ms = 0.f;
-        FTLM_CUDA(cudaEventElapsedTime(&ms, pr.first, pr.second));
-        c.prof.hv_ms += ms;
-        c.prof.hv_launches += 1;
-        cudaEventDestroy(pr.first);
-        cudaEventDestroy(pr.second);
-      }
-      float ms = 0.f;
-      FTLM_CUDA(cudaEventElapsedTime(&ms, ee0, ee1));
-      c.prof.eig_ms += ms;
-      cudaEventDestroy(ee0);
-      cudaEventDestroy(ee1);
-    }
+    c.prof.kernel_launches += 1;
     if (c.timing) {
       // algorithmic bytes per H*V launch: D*[nv*s*(1 + h_nz) + nv*s + m],
       // h_nz*D = nonzero-amplitude hops to active targets, m = 8 B per row
       const double s = fp32 ? 8.0 : 16.0;
-      const double nzh = static_cast<double>(block_nonzero_hops(c));
-      const double per = static_cast<double>(D) * nva * s * 2.0 + nzh * nva * s + static_cast<double>(D) * 8.0;
-      c.prof.hv_bytes += per * static_cast<double>(K);
+      hv_bytes += (static_cast<double>(D) * nva * s * 2.0 + nzh * nva * s + static_cast<double>(D) * 8.0) * K;
     }
     c.last_kdim = K;
     c.last_nv = NV;
-    pos += cnt;
+  }
+  // Ritz values and weights of all sweeps in one batched launch
+  cudaEvent_t ee0 = nullptr, ee1 = nullptr;
+  if (c.timing) {
+    FTLM_CUDA(cudaEventCreate(&ee0));
+    FTLM_CUDA(cudaEventCreate(&ee1));
+    FTLM_CUDA(cudaEventRecord(ee0, c.stream));
+  }
+  const size_t tsmem = sizeof(double) * 3 * 32 * static_cast<size_t>(K);
+  const int use_smem = tsmem <= 200 * 1024;
+  if (use_smem && tsmem > 48 * 1024)
+    FTLM_CUDA(cudaFuncSetAttribute(k_tridiag, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(tsmem)));
+  k_tridiag<<<(R + 31) / 32, 32, use_smem ? tsmem : 0, c.stream>>>(R, nvmax, ld, K, c.lz_alpha.as<double>(),
+                                                                  c.lz_beta.as<double>(), steps_all, dtmp, ztmp, etmp,
+                                                                  1.0 / R, status, use_smem);
+  if (c.timing) FTLM_CUDA(cudaEventRecord(ee1, c.stream));
+  k_compact<<<1, 256, sizeof(int) * (R + 1), c.stream>>>(R, K, steps_all, dtmp, ztmp, c.spectra.as<double>() + off,
+                                                          c.spectra.as<double>() + off + static_cast<int64_t>(R) * K,
+                                                          total);
+  FTLM_LAUNCH_CHECK();
+  c.prof.kernel_launches += 2;
+  int64_t cnt = 0;
+  int hstatus = 0;
+  FTLM_CUDA(cudaMemcpyAsync(&cnt, total, sizeof(int64_t), cudaMemcpyDeviceToHost, c.stream));
+  FTLM_CUDA(cudaMemcpyAsync(&hstatus, status, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  if (alpha_out) {
+    std::vector<double> a(static_cast<size_t>(nsweep) * K * ld), b(a.size());
+    std::vector<int32_t> sv(R);
+    FTLM_CUDA(cudaMemcpyAsync(a.data(), c.lz_alpha.p, sizeof(double) * a.size(), cudaMemcpyDeviceToHost, c.stream));
+    FTLM_CUDA(cudaMemcpyAsync(b.data(), c.lz_beta.p, sizeof(double) * b.size(), cudaMemcpyDeviceToHost, c.stream));
+    FTLM_CUDA(cudaMemcpyAsync(sv.data(), steps_all, sizeof(int32_t) * R, cudaMemcpyDeviceToHost, c.stream));
+    FTLM_CUDA(cudaStreamSynchronize(c.stream));
+    const int L = c.opts.lanczos_steps;
+    for (int r = 0; r < R; ++r) {
+      const int n = sv[r];
+      const size_t base = (static_cast<size_t>(r / nvmax) * K) * ld + r % nvmax;
+      (*steps_out)[r] = n;
+      for (int j = 0; j < n; ++j) (*alpha_out)[static_cast<size_t>(r) * L + j] = a[base + static_cast<size_t>(j) * ld];
+      for (int j = 0; j + 1 < n; ++j) (*beta_out)[static_cast<size_t>(r) * L + j] = b[base + static_cast<size_t>(j) * ld];
+    }
+  }
+  FTLM_CUDA(cudaStreamSynchronize(c.stream));
+  if (hstatus) throw Error(FTLM_ERR_NUMERIC, "tridiagonal QL did not converge");
+  if (c.timing) {
+    for (auto& pr : evs) {
+      float ms = 0.f;
+      FTLM_CUDA(cudaEventElapsedTime(&ms, pr.first, pr.second));
+      c.prof.hv_ms += ms;
+      c.prof.hv_launches += 1;
+      cudaEventDestroy(pr.first);
+      cudaEventDestroy(pr.second);
+    }
+    float ms = 0.f;
+    FTLM_CUDA(cudaEventElapsedTime(&ms, ee0, ee1));
+    c.prof.eig_ms += ms;
+    cudaEventDestroy(ee0);
+    cudaEventDestroy(ee1);
+    c.prof.hv_bytes += hv_bytes;
   }
   out.ev_off = off;
   out.w_off = off + static_cast<int64_t>(R) * K;
-  out.count = pos;
+  out.count = cnt;
   out.exact = false;
   out.prefactor = static_cast<double>(D);
   out.particles = n_up + n_dn;

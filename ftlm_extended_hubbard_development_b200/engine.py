@@ -55,7 +55,8 @@ class _Profile(C.Structure):
                 ("update_ms", C.c_double), ("update_launches", C.c_int64),
                 ("eig_ms", C.c_double), ("dense_ms", C.c_double), ("thermo_ms", C.c_double),
                 ("sector_ms", C.c_double), ("block_ms", C.c_double),
-                ("kernel_launches", C.c_int64), ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64)]
+                ("kernel_launches", C.c_int64), ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64),
+                ("hv_variant", C.c_int32), ("tune_runs", C.c_int32)]
 
 
 EXPORTS = [

@@ -80,6 +80,8 @@ typedef struct ftlm_profile {
   double eig_ms, dense_ms, thermo_ms, sector_ms, block_ms;
   int64_t kernel_launches; /* kernels of this library launched since the last reset */
   int64_t h2d_bytes, d2h_bytes;
+  int32_t hv_variant;      /* H*V kernel variant used last (autotuned unless FTLM_HV_VARIANT is set) */
+  int32_t tune_runs;       /* autotuner measurements made */
 } ftlm_profile;
 
 typedef struct ftlm_ctx ftlm_ctx;
