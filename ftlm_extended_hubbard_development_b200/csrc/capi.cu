@@ -132,6 +132,8 @@ int ftlm_ctx_create(const ftlm_model* model, const ftlm_run_opts* opts, ftlm_ctx
   c.device = opts->device;
   c.wide = model->lx * model->ly > 32;
   if (const char* hv = std::getenv("FTLM_HV_VARIANT")) c.hv_forced = std::atoi(hv);
+  if (const char* hm = std::getenv("FTLM_HV_MODE"))
+    c.hv_mode = std::string(hm) == "list" ? 1 : (std::string(hm) == "fly" ? 0 : -1);
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0 || c.device < 0 || c.device >= ndev) {
     cudaGetLastError();
@@ -164,7 +166,7 @@ void ftlm_ctx_destroy(ftlm_ctx* ctx) {
                         &c.blk.row_meta, &c.blk.row_dn, &c.vec_a, &c.vec_b, &c.vec_h, &c.partial,
                         &c.lz_alpha, &c.lz_beta, &c.lz_scale, &c.lz_state, &c.host_start, &c.ritz_tmp,
                         &c.scan_tmp, &c.dense_arena, &c.dense_meta, &c.dense_out, &c.spectra, &c.th_beta,
-                        &c.th_mu, &c.th_state};
+                        &c.th_mu, &c.th_state, &c.hl_ptr, &c.hl_ent};
   for (auto* b : bufs) b->release();
   if (c.stream) cudaStreamDestroy(c.stream);
   delete ctx;

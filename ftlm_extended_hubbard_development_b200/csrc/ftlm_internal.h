@@ -146,6 +146,10 @@ struct Ctx {
   Geom geom{};
   bool wide = false;  // 64-bit spin words (more than 32 sites)
   int hv_forced = -1; // H*V kernel variant forced by FTLM_HV_VARIANT (-1: autotune)
+  int hv_mode = -1;   // H*V operator source: -1 auto, 0 on-the-fly lookups, 1 cached hop list (FTLM_HV_MODE)
+  bool hl_active = false;  // H*V kernels read the cached hop list of the prepared block
+  int64_t hl_nnz = 0;
+  DBuf hl_ptr, hl_ent;     // hop list: int64 row pointers, packed uint64 entries
   int device = 0;
   int sm_count = 148;
   cudaStream_t stream = nullptr;
@@ -210,6 +214,8 @@ void reference_start_vectors(uint64_t bseed, int sample0, int nva, int64_t dim, 
 // Nonzero-amplitude hops with active targets in the prepared block (the
 // h_nz * dim of the H*V byte model).
 int64_t block_nonzero_hops(Ctx& c);
+// Builds the cached hop list of the prepared block; false when it does not fit in memory.
+bool hoplist_build(Ctx& c);
 
 // Spectra arena
 int64_t spectra_alloc(Ctx& c, int64_t count);  // returns offset (doubles) of 2*count slots

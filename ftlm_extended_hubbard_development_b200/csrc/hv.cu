@@ -261,6 +261,49 @@ __device__ __forceinline__ double2 finish_row(const double2& x, const double2& a
   return y;
 }
 
+// Gathers of one batch of nb <= 32 hops, whose (column, coefficient) lane
+// q holds for hop q: groups of G lanes take hops grp, grp+HPAR, ..., U hops
+// per group per iteration with all their loads issued before any FMA
+// (U*LPL 16-byte gathers in flight per lane). Summation order per lane is
+// the hop order, independent of U.
+template <typename T, int NV, int U>
+__device__ __forceinline__ void gather_batch(const typename CT<T>::V* __restrict__ in, int64_t col, T cr, T ci,
+                                             int nb,
+                                             typename CT<T>::V (&acc)[(NV / CT<T>::VPL < 32 ? 1 : NV / CT<T>::VPL / 32)]) {
+  using V = typename CT<T>::V;
+  constexpr int CPR = NV / CT<T>::VPL;
+  constexpr int G = CPR < 32 ? CPR : 32;
+  constexpr int LPL = CPR / G;
+  constexpr int HPAR = 32 / G;
+  const int lane = threadIdx.x & 31;
+  const int grp = lane / G;
+  const int sub = lane % G;
+  for (int j = 0; j < nb; j += HPAR * U) {
+    int64_t c[U];
+    T r[U], i[U];
+    V x[U][LPL];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int q = j + u * HPAR + grp;
+      c[u] = __shfl_sync(0xffffffffu, col, q & 31);
+      r[u] = __shfl_sync(0xffffffffu, cr, q & 31);
+      i[u] = __shfl_sync(0xffffffffu, ci, q & 31);
+      if (q >= nb) c[u] = -1;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+#pragma unroll
+      for (int l = 0; l < LPL; ++l) {
+        if (c[u] >= 0) x[u][l] = ld_stream(in + c[u] * CPR + l * G + sub);
+        else vzero(x[u][l]);
+      }
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+#pragma unroll
+      for (int l = 0; l < LPL; ++l) cfma<T>(acc[l], r[u], i[u], x[u][l]);
+  }
+}
+
 // H*V over all rows of the block. in/out: [dim][NV] complex T as 16-byte
 // chunks. scale[v] multiplies the result of vector v (Lanczos vectors are
 // stored unnormalised). partial[block][NV] receives Re<s*in, out> sums
@@ -390,33 +433,7 @@ __global__ void __launch_bounds__(kHvThreads, MINB) k_hv(const __grid_constant__
           ci = static_cast<T>((ar * pi + ai * pr) * ratio);
         }
       }
-      const int nb = min(32, total - b);
-      for (int j = 0; j < nb; j += HPAR * U) {
-        // U hops per lane group: all their loads are issued before any FMA,
-        // keeping U*LPL 16-byte gathers in flight per lane
-        int64_t c[U];
-        T r[U], i[U];
-        V x[U][LPL];
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-          const int q = j + u * HPAR + grp;
-          c[u] = __shfl_sync(0xffffffffu, col, q & 31);
-          r[u] = __shfl_sync(0xffffffffu, cr, q & 31);
-          i[u] = __shfl_sync(0xffffffffu, ci, q & 31);
-          if (q >= nb) c[u] = -1;
-        }
-#pragma unroll
-        for (int u = 0; u < U; ++u)
-#pragma unroll
-          for (int l = 0; l < LPL; ++l) {
-            if (c[u] >= 0) x[u][l] = ld_stream(in + c[u] * CPR + l * G + sub);
-            else vzero(x[u][l]);
-          }
-#pragma unroll
-        for (int u = 0; u < U; ++u)
-#pragma unroll
-          for (int l = 0; l < LPL; ++l) cfma<T>(acc[l], r[u], i[u], x[u][l]);
-      }
+      gather_batch<T, NV, U>(in, col, cr, ci, min(32, total - b), acc);
     }
     __syncwarp();
     // 3) fold the HPAR partial sums
@@ -451,6 +468,163 @@ __global__ void __launch_bounds__(kHvThreads, MINB) k_hv(const __grid_constant__
   }
 }
 
+// ------------------------------------------------------- cached hop list
+//
+// The alternative to recomputing every target lookup at every Lanczos step:
+// resolve the block's hops once into packed 8-byte entries
+//   col(32) | dir(3)<<32 | sign parity(1)<<35 | shift(6)<<36 | deg_t(7)<<42
+// (nonzero-amplitude hops to active targets, rows contiguous, int64 row
+// pointers) and stream them. The coefficient is rebuilt from the direction
+// amplitude, momentum phase and orbit sizes with a few FLOPs. Entries are in
+// the on-the-fly kernel's hop order (spin, source site, direction), so both
+// sources give identical sums.
+
+__device__ __forceinline__ uint64_t pack_hop(uint32_t col, int dir, int par, int shift, int deg) {
+  return static_cast<uint64_t>(col) | (static_cast<uint64_t>(dir) << 32) | (static_cast<uint64_t>(par) << 35) |
+         (static_cast<uint64_t>(shift) << 36) | (static_cast<uint64_t>(deg) << 42);
+}
+
+template <typename W>
+__global__ void k_hoplist(const __grid_constant__ CsrParams<W> P, const uint64_t* __restrict__ binom,
+                          const int64_t* __restrict__ row_ptr, uint64_t* __restrict__ hops) {
+  const Geom& g = P.g;
+  const BlockView<W>& v = P.v;
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < v.dim;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const uint32_t ur = v.row_meta[i] & 0x3FFFFFFu;
+    const W u = v.ur_bits[ur];
+    const W d = v.row_dn[i];
+    int64_t pos = row_ptr[i];
+    for (int spin = 0; spin < 2; ++spin) {
+      const W bits = spin ? d : u;
+      for (W m = bits; m; m &= m - 1) {
+        const int from = ctz(m);
+        for (int dir = 0; dir < 8; ++dir) {  // same filter as the nonzero-hop count pass
+          const int to = g.nb[from][dir];
+          if ((bits >> to) & 1) continue;
+          if (g.amp_re[dir] == 0.0 && g.amp_im[dir] == 0.0) continue;
+          const W moved = bits ^ (static_cast<W>(1) << from) ^ (static_cast<W>(1) << to);
+          int64_t c;
+          int shift, sgn, deg_t;
+          if (!resolve<W, uint64_t>(spin ? u : moved, spin ? moved : d, spin == 0, ur, v, g, binom, c, shift, sgn,
+                                    deg_t))
+            continue;
+          hops[pos++] = pack_hop(static_cast<uint32_t>(c), dir, jw_parity(bits, from, to) ^ sgn, shift, deg_t);
+        }
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ uint64_t ld_stream_u64(const uint64_t* p) {
+  uint64_t r;
+  asm("ld.global.nc.L1::no_allocate.u64 %0, [%1];" : "=l"(r) : "l"(p));
+  return r;
+}
+
+// H*V from the cached hop list (same contract as k_hv).
+template <typename W, typename T, int NV, int U, int MINB>
+__global__ void __launch_bounds__(kHvThreads, MINB) k_hv_list(const __grid_constant__ HvParams<W> P,
+                                                              const int64_t* __restrict__ hptr,
+                                                              const uint64_t* __restrict__ hops,
+                                                              const typename CT<T>::V* __restrict__ in,
+                                                              typename CT<T>::V* __restrict__ out,
+                                                              const double* __restrict__ scale,
+                                                              double* __restrict__ partial) {
+  using V = typename CT<T>::V;
+  constexpr int VPL = CT<T>::VPL;
+  constexpr int CPR = NV / VPL;
+  constexpr int G = CPR < 32 ? CPR : 32;
+  constexpr int LPL = CPR / G;
+  __shared__ double s_ph[2][64];
+  __shared__ double s_amp[2][8];
+  __shared__ double s_sq[65];
+  __shared__ double s_dot[kHvWarps][NV];
+  const Geom& g = P.g;
+  const BlockView<W>& v = P.v;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < 64; i += kHvThreads) {
+    s_ph[0][i] = v.phase_re[i];
+    s_ph[1][i] = v.phase_im[i];
+  }
+  if (tid < 8) {
+    s_amp[0][tid] = g.amp_re[tid];
+    s_amp[1][tid] = g.amp_im[tid];
+  }
+  if (tid < 65) s_sq[tid] = g.sqrt_deg[tid];
+  __syncthreads();
+  const int lane = tid & 31;
+  const int wid = tid >> 5;
+  const int grp = lane / G;
+  const int sub = lane % G;
+  double sc[LPL][VPL];
+  double dot[LPL][VPL];
+#pragma unroll
+  for (int l = 0; l < LPL; ++l)
+#pragma unroll
+    for (int e = 0; e < VPL; ++e) {
+      sc[l][e] = scale ? scale[(l * G + sub) * VPL + e] : 1.0;
+      dot[l][e] = 0.0;
+    }
+  const int64_t nwarps = static_cast<int64_t>(gridDim.x) * kHvWarps;
+  for (int64_t row = static_cast<int64_t>(blockIdx.x) * kHvWarps + wid; row < v.dim; row += nwarps) {
+    const uint32_t meta = __ldg(v.row_meta + row);
+    const double inv_s = 1.0 / s_sq[static_cast<int>(meta >> 26) + 1];
+    const int64_t h0 = __ldg(hptr + row), h1 = __ldg(hptr + row + 1);
+    V acc[LPL];
+#pragma unroll
+    for (int l = 0; l < LPL; ++l) vzero(acc[l]);
+    for (int64_t b = h0; b < h1; b += 32) {
+      const int64_t q = b + lane;
+      int64_t col = -1;
+      T cr = 0, ci = 0;
+      if (q < h1) {
+        const uint64_t e = ld_stream_u64(hops + q);
+        col = static_cast<int64_t>(static_cast<uint32_t>(e));
+        const int dir = static_cast<int>((e >> 32) & 7);
+        const int p = static_cast<int>((e >> 35) & 1);
+        const int shift = static_cast<int>((e >> 36) & 63);
+        const int deg_t = static_cast<int>((e >> 42) & 127);
+        const double ar = p ? -s_amp[0][dir] : s_amp[0][dir];
+        const double ai = p ? -s_amp[1][dir] : s_amp[1][dir];
+        const double pr = s_ph[0][shift], pi = s_ph[1][shift];
+        const double ratio = s_sq[deg_t] * inv_s;
+        cr = static_cast<T>((ar * pr - ai * pi) * ratio);
+        ci = static_cast<T>((ar * pi + ai * pr) * ratio);
+      }
+      gather_batch<T, NV, U>(in, col, cr, ci, static_cast<int>(min(static_cast<int64_t>(32), h1 - b)), acc);
+    }
+#pragma unroll
+    for (int o = G; o < 32; o <<= 1)
+#pragma unroll
+      for (int l = 0; l < LPL; ++l) vadd(acc[l], shfl_xor_v(acc[l], o));
+    if (grp == 0) {
+      const W u = __ldg(v.ur_bits + (meta & 0x3FFFFFFu));
+      const W d = __ldg(v.row_dn + row);
+      const double diag = diag_energy(u, d, g);
+#pragma unroll
+      for (int l = 0; l < LPL; ++l) {
+        const V x = ld_stream(in + row * CPR + l * G + sub);
+        out[row * CPR + l * G + sub] = finish_row(x, acc[l], diag, sc[l], dot[l]);
+      }
+    }
+  }
+  if (partial) {
+    if (grp == 0) {
+#pragma unroll
+      for (int l = 0; l < LPL; ++l)
+#pragma unroll
+        for (int e = 0; e < VPL; ++e) s_dot[wid][(l * G + sub) * VPL + e] = dot[l][e];
+    }
+    __syncthreads();
+    for (int vv = tid; vv < NV; vv += kHvThreads) {
+      double s = 0.0;
+      for (int w = 0; w < kHvWarps; ++w) s += s_dot[w][vv];
+      partial[static_cast<int64_t>(blockIdx.x) * NV + vv] = s;
+    }
+  }
+}
+
 template <typename W, typename R, typename T, int NV, int U, int MINB>
 void launch_hv_t(Ctx& c, const void* in, void* out, const double* scale, double* partial, int grid) {
   HvParams<W> P;
@@ -458,6 +632,12 @@ void launch_hv_t(Ctx& c, const void* in, void* out, const double* scale, double*
   if constexpr (sizeof(W) == 4) P.v = view32(c);
   else P.v = view64(c);
   using V = typename CT<T>::V;
+  if (c.hl_active) {
+    k_hv_list<W, T, NV, U, MINB><<<grid, kHvThreads, 0, c.stream>>>(P, c.hl_ptr.as<int64_t>(), c.hl_ent.as<uint64_t>(),
+                                                                    static_cast<const V*>(in), static_cast<V*>(out),
+                                                                    scale, partial);
+    return;
+  }
   const R* gb = sizeof(R) == 4 ? reinterpret_cast<const R*>(c.binom32.p) : reinterpret_cast<const R*>(c.binom.p);
   k_hv<W, R, T, NV, U, MINB><<<grid, kHvThreads, 0, c.stream>>>(P, static_cast<const V*>(in), static_cast<V*>(out),
                                                                 scale, partial, gb);
@@ -576,7 +756,42 @@ int64_t block_nonzero_hops_t(Ctx& c) {
   return scan_excl_i32_to_i64(c, cnt.as<int32_t>(), rp64.as<int64_t>(), D);
 }
 
+template <typename W>
+bool hoplist_build_t(Ctx& c) {
+  const int64_t D = c.blk.dim;
+  if (D <= 0) return false;
+  CsrParams<W> P;
+  P.g = c.geom;
+  if constexpr (sizeof(W) == 4) P.v = view32(c);
+  else P.v = view64(c);
+  DBuf& cnt = c.sec.tmp_a;
+  cnt.ensure(sizeof(int32_t) * D);
+  k_csr<W><<<grid_for(D, 128), 128, 0, c.stream>>>(P, c.binom.as<uint64_t>(), 2, cnt.as<int32_t>(), nullptr, nullptr,
+                                                    nullptr, nullptr);
+  FTLM_LAUNCH_CHECK();
+  c.hl_ptr.ensure(sizeof(int64_t) * (D + 1));
+  const int64_t nnz = scan_excl_i32_to_i64(c, cnt.as<int32_t>(), c.hl_ptr.as<int64_t>(), D);
+  FTLM_CUDA(cudaMemcpyAsync(c.hl_ptr.as<int64_t>() + D, &nnz, sizeof(int64_t), cudaMemcpyHostToDevice, c.stream));
+  size_t free_b = 0, total_b = 0;
+  FTLM_CUDA(cudaMemGetInfo(&free_b, &total_b));
+  const size_t need = sizeof(uint64_t) * static_cast<size_t>(std::max<int64_t>(nnz, 1));
+  if (need > c.hl_ent.cap && need + (size_t(2) << 30) > free_b + c.hl_ent.cap) return false;  // keep 2 GiB headroom
+  c.hl_ent.ensure(need);
+  k_hoplist<W><<<grid_for(D, 128), 128, 0, c.stream>>>(P, c.binom.as<uint64_t>(), c.hl_ptr.as<int64_t>(),
+                                                        c.hl_ent.as<uint64_t>());
+  FTLM_LAUNCH_CHECK();
+  FTLM_CUDA(cudaStreamSynchronize(c.stream));
+  c.prof.kernel_launches += 5;
+  c.hl_nnz = nnz;
+  return true;
+}
+
 }  // namespace
+
+bool hoplist_build(Ctx& c) {
+  if (c.wide) return hoplist_build_t<uint64_t>(c);
+  return hoplist_build_t<uint32_t>(c);
+}
 
 int64_t block_nonzero_hops(Ctx& c) {
   if (c.wide) return block_nonzero_hops_t<uint64_t>(c);
@@ -625,7 +840,8 @@ int hv_grid(Ctx& c, int nv, bool fp32) {
 
 int hv_variant(Ctx& c, const void* in, void* out, int nv, bool fp32, int grid) {
   if (c.hv_forced >= 0 && c.hv_forced < kNumVariants) return c.hv_forced;
-  const auto key = std::make_tuple(c.wide ? 1 : 0, fp32 ? 1 : 0, nv, size_class(c.blk.dim), c.device);
+  const auto key = std::make_tuple((c.wide ? 1 : 0) | (c.hl_active ? 2 : 0), fp32 ? 1 : 0, nv, size_class(c.blk.dim),
+                                   c.device);
   {
     std::lock_guard<std::mutex> lock(g_tune_mu);
     auto it = g_tuned.find(key);

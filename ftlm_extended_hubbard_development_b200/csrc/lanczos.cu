@@ -470,7 +470,17 @@ void run_ftlm_block(Ctx& c, int n_up, int n_dn, int mx, int my, Spectrum& out, c
   std::vector<double> hstart;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> evs;
   double hv_bytes = 0.0;
-  const double nzh = c.timing ? static_cast<double>(block_nonzero_hops(c)) : 0.0;
+  // Operator source: the cached hop list pays one lookup pass per block and
+  // then streams 8 B per hop; it pays off when few vectors share each lookup.
+  struct ListGuard {
+    Ctx& c;
+    ~ListGuard() { c.hl_active = false; }
+  } guard{c};
+  bool use_list = c.hv_mode == 1 ||
+                  (c.hv_mode < 0 && D >= (1 << 14) && next_pow2(std::min(nvmax, R)) <= (fp32 ? 32 : 16));
+  if (use_list) use_list = hoplist_build(c);
+  c.hl_active = use_list;
+  const double nzh = c.timing ? static_cast<double>(use_list ? c.hl_nnz : block_nonzero_hops(c)) : 0.0;
   for (int s0 = 0; s0 < R; s0 += nvmax) {
     const int nva = std::min(nvmax, R - s0);
     const int NV = next_pow2(std::max(nva, fp32 ? 2 : 1));

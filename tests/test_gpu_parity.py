@@ -181,6 +181,23 @@ def test_profile_counters_and_byte_model(golden):
     assert p["kernel_launches"] >= 4 * K
 
 
+@pytest.mark.parametrize("prec,batch", [(E.PREC_FP64, 1), (E.PREC_MIXED, 16), (E.PREC_FP64, 4)])
+def test_cached_hop_list_equals_on_the_fly(golden, monkeypatch, prec, batch):
+    """The cached hop list resolves the same hops in the same order with the
+    same coefficient arithmetic as the on-the-fly kernel: identical results."""
+    m = model_of(golden, "c4x4")
+    opts = pkg.RunOpts(samples=4, lanczos_steps=30, precision=prec, batch_vectors=batch,
+                       start_vector=E.START_PHILOX_PHASE)
+    out = {}
+    for mode in ("fly", "list"):
+        monkeypatch.setenv("FTLM_HV_MODE", mode)
+        with pkg.Engine(m, opts) as eng:
+            eng.sector_prepare(2, 3)
+            out[mode] = eng.block_lanczos(1, 2)
+    for a, b in zip(out["fly"], out["list"]):
+        assert np.array_equal(a, b)
+
+
 def test_exact_eigenvalues_match_reference(golden):
     for case, nu, nd, mx, my in golden.meta["exact_dumps"]:
         m = model_of(golden, case)
