@@ -66,6 +66,9 @@ EXPORTS = [
     "ftlm_thermo_read", "ftlm_block_apply", "ftlm_block_lanczos",
     "ftlm_debug_sector_parents", "ftlm_debug_sector_relations", "ftlm_debug_block_csr",
     "ftlm_profile_enable", "ftlm_profile_read", "ftlm_profile_reset", "ftlm_ritz_noalloc",
+    "ftlm_mlp_create", "ftlm_mlp_destroy", "ftlm_mlp_last_error", "ftlm_mlp_num_params",
+    "ftlm_mlp_get_params", "ftlm_mlp_set_params", "ftlm_mlp_forward", "ftlm_mlp_loss_grad",
+    "ftlm_mlp_train",
 ]
 
 _lib = None
@@ -102,6 +105,15 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "ftlm_profile_read": ([vp, P(_Profile)], C.c_int),
         "ftlm_profile_reset": ([vp], C.c_int),
         "ftlm_ritz_noalloc": ([vp, vp, vp, i32, i32, d, vp, vp, vp, vp, C.c_char_p, sz], C.c_int),
+        "ftlm_mlp_create": ([i32, i32, i32, i32, u64, i32, P(vp)], C.c_int),
+        "ftlm_mlp_destroy": ([vp], None),
+        "ftlm_mlp_last_error": ([vp, C.c_char_p, sz], C.c_int),
+        "ftlm_mlp_num_params": ([vp, P(C.c_int64)], C.c_int),
+        "ftlm_mlp_get_params": ([vp, vp, C.c_int64], C.c_int),
+        "ftlm_mlp_set_params": ([vp, vp, C.c_int64], C.c_int),
+        "ftlm_mlp_forward": ([vp, vp, C.c_int64, vp], C.c_int),
+        "ftlm_mlp_loss_grad": ([vp, vp, vp, vp, C.c_int64, P(C.c_float), vp], C.c_int),
+        "ftlm_mlp_train": ([vp, vp, vp, vp, C.c_int64, i32, i32, C.c_float, u64, vp], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -345,3 +357,74 @@ def run_curve(model: Model, betas, mu, opts: RunOpts | None = None, ed: bool = F
     chi = np.maximum(0.0, (n2 / z - mean * mean) / n)
     return {"n": mean / n, "charge_correlation": chi, "compressibility": b * chi,
             "partition_like": z, "log_partition": np.log(z) - b * emin}
+
+
+class Mlp:
+    """The twist-surrogate network (ftlm_mlp): FP32 MLP trained on the GPU by
+    the library's own forward/backward/Adam kernels."""
+
+    def __init__(self, n_in: int, width: int, depth: int, n_out: int, seed: int = 1234,
+                 device: int = 0):
+        self.lib = load_library()
+        h = C.c_void_p()
+        st = self.lib.ftlm_mlp_create(n_in, width, depth, n_out, seed, device, C.byref(h))
+        if st != OK:
+            raise FtlmError(st, "ftlm_mlp_create failed")
+        self.h = h
+        self.n_in, self.width, self.depth, self.n_out = n_in, width, depth, n_out
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.ftlm_mlp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st: int):
+        if st != OK:
+            buf = C.create_string_buffer(512)
+            self.lib.ftlm_mlp_last_error(self.h, buf, 512)
+            raise FtlmError(st, buf.value.decode())
+
+    @property
+    def num_params(self) -> int:
+        n = C.c_int64(0)
+        self._check(self.lib.ftlm_mlp_num_params(self.h, C.byref(n)))
+        return n.value
+
+    def get_params(self) -> np.ndarray:
+        p = np.zeros(self.num_params, np.float32)
+        self._check(self.lib.ftlm_mlp_get_params(self.h, _p(p), len(p)))
+        return p
+
+    def set_params(self, p: np.ndarray):
+        p = np.ascontiguousarray(p, np.float32)
+        self._check(self.lib.ftlm_mlp_set_params(self.h, _p(p), len(p)))
+
+    def forward(self, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.zeros((x.shape[0], self.n_out), np.float32)
+        self._check(self.lib.ftlm_mlp_forward(self.h, _p(x), x.shape[0], _p(y)))
+        return y
+
+    def loss_grad(self, x, t, mask):
+        x = np.ascontiguousarray(x, np.float32)
+        t = np.ascontiguousarray(t, np.float32)
+        m = np.ascontiguousarray(mask, np.float32)
+        loss = C.c_float(0.0)
+        g = np.zeros(self.num_params, np.float32)
+        self._check(self.lib.ftlm_mlp_loss_grad(self.h, _p(x), _p(t), _p(m), x.shape[0], C.byref(loss), _p(g)))
+        return loss.value, g
+
+    def train(self, x, t, mask, epochs: int, batch: int, lr: float, seed: int = 7) -> np.ndarray:
+        x = np.ascontiguousarray(x, np.float32)
+        t = np.ascontiguousarray(t, np.float32)
+        m = np.ascontiguousarray(mask, np.float32)
+        hist = np.zeros(epochs, np.float32)
+        self._check(self.lib.ftlm_mlp_train(self.h, _p(x), _p(t), _p(m), x.shape[0], epochs, batch, lr,
+                                            seed, _p(hist)))
+        return hist

@@ -1,0 +1,287 @@
+"""Learned twist surrogate: per-block low-lying spectra as a function of twist.
+
+A small FP32 MLP (engine.Mlp, trained on the GPU by the library's own
+forward / backward / Adam kernels) maps a block's twist and quantum numbers
+(phi_x, phi_y, N_up, N_down, k_x, k_y) to the block's `levels` lowest energy
+levels and their trace weights. Its training data are the spectra the GPU
+engine itself produces on a uniform grid of twists. From the predicted levels
+the surrogate proposes the n(mu) curve at any twist, e.g. on a dense grid for
+the twist average. Plain FTLM (or ED) at held-out twists is its judge: when
+the surrogate's n(mu) there is off by more than the threshold, the twist
+average falls back to the engine's own twists.
+
+Per block and twist the spectrum is split in two:
+  * low part - the block spectrum sorted and merged into levels (Ritz values
+    of different random vectors that agree to `tol`, and degenerate
+    eigenvalues), each with its total trace weight (prefactor * summed FTLM
+    weights, or the multiplicity for an exact block); the lowest `levels` of
+    them are the network's targets, masked where the block has fewer;
+  * tail - everything above, kept only as its partition sum per beta,
+    log sum_i w_i exp(-beta e_i).
+A proposal at twist phi takes the low part from the network and the tail of
+the training twist nearest to phi, so truncating the spectrum costs nothing
+at the training twists and little elsewhere. The network learns the twist
+dependence on top of a per-(block, level) mean over the training twists, so
+its output is a small correction with unit-scaled targets.
+
+A block's spectrum is not periodic with period 1 in phi: the gauge change
+that removes one flux quantum moves the block to momentum k + N. The inputs
+therefore carry the per-bond phase 2 pi phi / L beside 2 pi phi.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, replace
+
+import numpy as np
+
+from .engine import Engine, Mlp, Model, RunOpts
+from .twist import combine_rows, curve_rows, uniform_grid
+
+LEVELS = 16
+N_FEAT = 14
+
+
+def block_features(phix, phiy, nup, ndn, mx, my, lx, ly):
+    """Network input of one block at one twist: periodic quantities as
+    sin/cos pairs, particle numbers as fillings."""
+    t = 2.0 * math.pi
+    n = lx * ly
+    return [math.sin(t * phix), math.cos(t * phix), math.sin(t * phiy), math.cos(t * phiy),
+            math.sin(t * phix / lx), math.cos(t * phix / lx), math.sin(t * phiy / ly), math.cos(t * phiy / ly),
+            nup / n, ndn / n, math.cos(t * mx / lx), math.sin(t * mx / lx), math.cos(t * my / ly),
+            math.sin(t * my / ly)]
+
+
+def reduce_spectrum(ev, w, pref, exact, levels=LEVELS, tol=1e-6):
+    """Lowest `levels` merged levels (energy, trace weight, present mask) of a
+    block, and the remaining (energies, trace weights) as the tail."""
+    ev = np.asarray(ev, np.float64)
+    o = np.argsort(ev, kind="stable")
+    e = ev[o]
+    ww = np.ones_like(e) if exact or w is None else pref * np.asarray(w, np.float64)[o]
+    E = np.zeros(levels)
+    W = np.zeros(levels)
+    M = np.zeros(levels)
+    k = -1
+    cut = len(e)
+    for i in range(len(e)):
+        if k >= 0 and abs(e[i] - E[k]) <= tol * max(1.0, abs(E[k])):
+            W[k] += ww[i]
+            continue
+        if k + 1 >= levels:
+            cut = i
+            break
+        k += 1
+        E[k], W[k], M[k] = e[i], ww[i], 1.0
+    return E, W, M, e[cut:], ww[cut:]
+
+
+def tail_log_partition(e, w, betas):
+    """log sum_i w_i exp(-beta e_i) per beta (-inf for an empty tail)."""
+    out = np.full(len(betas), -np.inf)
+    keep = w > 0
+    e, w = e[keep], w[keep]
+    if len(e):
+        for ib, b in enumerate(betas):
+            a = np.log(w) - b * e
+            top = a.max()
+            out[ib] = top + math.log(np.exp(a - top).sum())
+    return out
+
+
+@dataclass
+class TwistData:
+    """Engine output at one twist: per block (nup, ndn, mx, my, particles,
+    E[levels], W[levels], M[levels], tail_logz[nbeta]) and the engine's own
+    n(mu) curve (dict of [nbeta][nmu] arrays)."""
+    phix: float
+    phiy: float
+    blocks: list
+    curve: dict
+
+
+def collect(model: Model, phix, phiy, betas, mu, opts: RunOpts, ed=False, levels=LEVELS) -> TwistData:
+    """Every block's spectrum and the n(mu) curve at one twist, in the
+    reference's (N_up, N_down, k) block order."""
+    eng = Engine(replace(model, phix=float(phix), phiy=float(phiy)), opts)
+    blocks = []
+    try:
+        eng.thermo_configure(betas, mu)
+        n = model.sites
+        for nu in range(n + 1):
+            for nd in range(n + 1):
+                info = eng.sector_prepare(nu, nd)
+                ks = [(k % model.lx, k // model.lx) for k, d in enumerate(info.block_dims) if d > 0]
+                exact = [b for b in ks
+                         if ed or info.block_dims[b[1] * model.lx + b[0]] <= opts.exact_block_threshold]
+                eng.blocks_exact_batched(exact)
+                for b in ks:
+                    is_exact = b in exact
+                    ev, w, pref = eng.block_spectrum(b[0], b[1], exact=is_exact)
+                    E, W, M, te, tw = reduce_spectrum(ev, w, pref, is_exact, levels)
+                    blocks.append((nu, nd, b[0], b[1], nu + nd, E, W, M, tail_log_partition(te, tw, betas)))
+                    eng.thermo_accumulate_block(*b)
+        emin, z, ns, n2 = eng.thermo_read()
+    finally:
+        eng.close()
+    bb = np.asarray(betas, np.float64).reshape(-1, 1)
+    mean = ns / z
+    chi = np.maximum(0.0, (n2 / z - mean * mean) / model.sites)
+    curve = {"n": mean / model.sites, "charge_correlation": chi, "compressibility": bb * chi,
+             "partition_like": z, "log_partition": np.log(z) - bb * emin}
+    return TwistData(float(phix), float(phiy), blocks, curve)
+
+
+def curve_from_blocks(blocks, sites, betas, mu):
+    """n(mu) observables from per-block levels plus tail partition sums; the
+    shifted log-sum-exp of the reference (main.cpp:1172-1219, 1770-1788)
+    with one shift per mu, the lowest level of any block minus mu * N."""
+    mu = np.asarray(mu, np.float64)
+    shift = np.full(len(mu), np.inf)
+    for b in blocks:
+        if b[7].any():
+            shift = np.minimum(shift, b[5][b[7] > 0].min() - mu * b[4])
+    out = {k: np.zeros((len(betas), len(mu))) for k in
+           ("n", "charge_correlation", "compressibility", "partition_like", "log_partition")}
+    for ib, beta in enumerate(betas):
+        z = np.zeros(len(mu))
+        n1 = np.zeros(len(mu))
+        n2 = np.zeros(len(mu))
+        for nu, nd, mx, my, p, E, W, M, tail in blocks:
+            sel = M > 0
+            zz = (W[sel, None] * np.exp(-beta * (E[sel, None] - mu[None, :] * p - shift[None, :]))).sum(0)
+            if np.isfinite(tail[ib]):
+                zz = zz + np.exp(tail[ib] + beta * (mu * p + shift))
+            z += zz
+            n1 += p * zz
+            n2 += p * p * zz
+        mean = n1 / z
+        chi = np.maximum(0.0, (n2 / z - mean * mean) / sites)
+        out["n"][ib] = mean / sites
+        out["charge_correlation"][ib] = chi
+        out["compressibility"][ib] = beta * chi
+        out["partition_like"][ib] = z
+        out["log_partition"][ib] = np.log(z) - beta * shift
+    return out
+
+
+def _dist2(a, b, wrap):
+    d = [abs(x - y) for x, y in zip(a, b)]
+    if wrap:
+        d = [min(x, 1.0 - x) for x in d]
+    return d[0] ** 2 + d[1] ** 2
+
+
+class TwistSurrogate:
+    """MLP over (twist, block quantum numbers) -> lowest levels and weights."""
+
+    def __init__(self, model: Model, levels=LEVELS, width=128, depth=3, seed=1234, device=0):
+        self.model = model
+        self.levels = levels
+        self.net = Mlp(N_FEAT, width, depth, 2 * levels, seed=seed, device=device)
+        self.keys = None
+        self.train_data = None
+
+    def close(self):
+        self.net.close()
+
+    def _tables(self, data):
+        keys = [b[:5] for b in data[0].blocks]
+        idx = {k: i for i, k in enumerate(keys)}
+        L = self.levels
+        E = np.zeros((len(data), len(keys), L))
+        W = np.zeros_like(E)
+        M = np.zeros_like(E)
+        for t, td in enumerate(data):
+            for b in td.blocks:
+                i = idx[b[:5]]
+                E[t, i], W[t, i], M[t, i] = b[5], b[6], b[7]
+        return keys, E, W, M
+
+    def features(self, phix, phiy):
+        lx, ly = self.model.lx, self.model.ly
+        return np.array([block_features(phix, phiy, k[0], k[1], k[2], k[3], lx, ly) for k in self.keys],
+                        np.float32)
+
+    def fit(self, data, epochs=1500, batch=512, lr=1e-3, seed=7):
+        """Train on the TwistData of the training twists; returns the loss
+        history (one value per epoch, Adam at lr, then a third as many epochs
+        at lr / 5)."""
+        self.train_data = data
+        self.keys, E, W, M = self._tables(data)
+        mcount = np.maximum(M.sum(0), 1.0)
+        self.mask = (M.sum(0) > 0).astype(np.float64)  # a level present at any training twist
+        self.e0 = (E * M).sum(0) / mcount
+        self.w0 = (W * M).sum(0) / mcount
+        rE = (E - self.e0) * M
+        rW = (W - self.w0) * M
+        cnt = max(M.sum(), 1.0)
+        self.se = max(float(np.sqrt((rE ** 2).sum() / cnt)), 1e-6)
+        self.sw = max(float(np.sqrt((rW ** 2).sum() / cnt)), 1e-6)
+        X = np.concatenate([self.features(td.phix, td.phiy) for td in data])
+        T = np.concatenate([np.concatenate([rE[t] / self.se, rW[t] / self.sw], 1) for t in range(len(data))])
+        Mk = np.concatenate([np.concatenate([M[t], M[t]], 1) for t in range(len(data))])
+        T, Mk = T.astype(np.float32), Mk.astype(np.float32)
+        h1 = self.net.train(X, T, Mk, epochs, batch, lr, seed)
+        h2 = self.net.train(X, T, Mk, max(epochs // 3, 1), batch, lr / 5, seed + 1)
+        return np.concatenate([h1, h2])
+
+    def nearest(self, phix, phiy, wrap=False):
+        return min(self.train_data, key=lambda t: _dist2((t.phix, t.phiy), (phix, phiy), wrap))
+
+    def predict_blocks(self, phix, phiy):
+        """Blocks at a twist: predicted low levels, nearest training tail."""
+        y = self.net.forward(self.features(phix, phiy)).astype(np.float64)
+        L = self.levels
+        E = self.e0 + y[:, :L] * self.se
+        W = np.maximum(self.w0 + y[:, L:] * self.sw, 0.0)
+        near = self.nearest(phix, phiy)
+        return [(*k, E[i], W[i], self.mask[i], near.blocks[i][8]) for i, k in enumerate(self.keys)]
+
+    def curve(self, phix, phiy, betas, mu):
+        return curve_from_blocks(self.predict_blocks(phix, phiy), self.model.sites, betas, mu)
+
+
+def heldout_twists(count=8, seed=2024):
+    """Held-out judge twists in [0, 1)^2 from a Philox generator of fixed seed."""
+    g = np.random.Generator(np.random.Philox(seed))
+    return [tuple(map(float, t)) for t in g.random((count, 2))]
+
+
+def surrogate_twist_average(model: Model, betas, mu, opts: RunOpts, grid=6, heldout=8, dense=24,
+                            threshold=0.01, ed=False, epochs=1500, seed=2024, levels=LEVELS, device=0):
+    """Train on a grid x grid twist set, judge at `heldout` Philox twists with
+    the engine, and average n(mu) over the surrogate's dense x dense grid when
+    every judge passes (max |dn| <= threshold); otherwise average the
+    engine's own curves at the training and held-out twists (fallback)."""
+    opts = replace(opts, device=device)
+    train = [collect(model, px, py, betas, mu, opts, ed, levels) for px, py in uniform_grid(grid)]
+    sur = TwistSurrogate(model, levels=levels, device=device)
+    hist = sur.fit(train, epochs=epochs)
+    judges = []
+    for px, py in heldout_twists(heldout, seed):
+        td = collect(model, px, py, betas, mu, opts, ed, levels)
+        pred = sur.curve(px, py, betas, mu)
+        near = sur.nearest(px, py, wrap=True)  # the curve without the network
+        judges.append({"twist": (px, py), "curve": td.curve,
+                       "err_surrogate": float(np.abs(pred["n"] - td.curve["n"]).max()),
+                       "err_nearest_twist": float(np.abs(near.curve["n"] - td.curve["n"]).max())})
+    accepted = all(j["err_surrogate"] <= threshold for j in judges)
+    rows = []
+    if accepted:
+        for px, py in uniform_grid(dense):
+            rows += curve_rows(sur.curve(px, py, betas, mu), betas, mu)
+        source = f"surrogate {dense}x{dense} grid"
+    else:
+        for td in train:
+            rows += curve_rows(td.curve, betas, mu)
+        for j in judges:
+            rows += curve_rows(j["curve"], betas, mu)
+        source = "engine twists (fallback)"
+    grid_rows = []
+    for td in train:
+        grid_rows += curve_rows(td.curve, betas, mu)
+    return {"average": combine_rows(rows, "observable-average"), "source": source, "accepted": accepted,
+            "judges": judges, "loss_history": hist, "training_grid_average": combine_rows(grid_rows),
+            "surrogate": sur, "train": train}

@@ -193,6 +193,32 @@ int ftlm_ritz_noalloc(const double* alpha, const double* beta, const int32_t* st
                       double inv_samples, double* evals, double* weights, int64_t* count, void* stream,
                       char* errbuf, size_t errlen);
 
+/* Twist-surrogate network (no counterpart in the reference: the learned part
+ * of the engine). An FP32 MLP, x[n_in] -> `depth` hidden tanh layers of
+ * `width` -> linear y[n_out], trained on the GPU by this library's own
+ * forward / backward / Adam kernels on a masked mean-squared error. Host
+ * arrays are row-major [n][n_in] / [n][n_out]. Parameters are one flat FP32
+ * vector, per layer W[out][in] then b[out]. */
+typedef struct ftlm_mlp ftlm_mlp;
+int ftlm_mlp_create(int32_t n_in, int32_t width, int32_t depth, int32_t n_out, uint64_t seed, int32_t device,
+                    ftlm_mlp** out);
+void ftlm_mlp_destroy(ftlm_mlp* net);
+int ftlm_mlp_last_error(const ftlm_mlp* net, char* buf, size_t len);
+int ftlm_mlp_num_params(const ftlm_mlp* net, int64_t* count);
+int ftlm_mlp_get_params(ftlm_mlp* net, float* host, int64_t count);
+int ftlm_mlp_set_params(ftlm_mlp* net, const float* host, int64_t count);
+/* Inference: y = f(x) for n rows. */
+int ftlm_mlp_forward(ftlm_mlp* net, const float* x, int64_t n, float* y);
+/* Loss sum(mask*(f(x)-t)^2)/sum(mask) and, if grad != NULL, its gradient
+ * w.r.t. the flat parameter vector (one forward + backward pass). */
+int ftlm_mlp_loss_grad(ftlm_mlp* net, const float* x, const float* t, const float* mask, int64_t n, float* loss,
+                       float* grad);
+/* Adam training: `epochs` shuffled passes of full mini-batches of `batch`
+ * rows (seeded shuffle); loss_history[epochs] (may be NULL) gets the mean
+ * batch loss of each epoch. */
+int ftlm_mlp_train(ftlm_mlp* net, const float* x, const float* t, const float* mask, int64_t n, int32_t epochs,
+                   int32_t batch, float lr, uint64_t seed, float* loss_history);
+
 /* Instrumentation: per-kernel CUDA-event timing (adds a sync per timed
  * launch), and the counters accumulated since the last reset. */
 int ftlm_profile_enable(ftlm_ctx* ctx, int32_t on);
