@@ -134,6 +134,7 @@ int ftlm_ctx_create(const ftlm_model* model, const ftlm_run_opts* opts, ftlm_ctx
   if (const char* hv = std::getenv("FTLM_HV_VARIANT")) c.hv_forced = std::atoi(hv);
   if (const char* hm = std::getenv("FTLM_HV_MODE"))
     c.hv_mode = std::string(hm) == "list" ? 1 : (std::string(hm) == "fly" ? 0 : -1);
+  if (const char* sb = std::getenv("FTLM_SMALL_BLOCKS")) c.small_blocks = std::string(sb) != "0";
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0 || c.device < 0 || c.device >= ndev) {
     cudaGetLastError();
@@ -164,7 +165,8 @@ void ftlm_ctx_destroy(ftlm_ctx* ctx) {
                         &c.sec.d_chi, &c.sec.d_cidx, &c.sec.canon, &c.sec.tmp_a, &c.sec.tmp_b, &c.sec.tmp_c,
                         &c.sec.tmp_d, &c.sec.tmp_e, &c.blk.act, &c.blk.act_list, &c.blk.aoff, &c.blk.dtab,
                         &c.blk.row_meta, &c.blk.row_dn, &c.vec_a, &c.vec_b, &c.vec_h, &c.partial,
-                        &c.lz_alpha, &c.lz_beta, &c.lz_scale, &c.lz_state, &c.host_start, &c.ritz_tmp,
+                        &c.lz_alpha, &c.lz_beta, &c.lz_scale, &c.lz_state, &c.host_start, &c.ritz_tmp, &c.ritz_out,
+                        &c.sb_rp, &c.sb_col, &c.sb_val, &c.sb_diag, &c.sb_meta, &c.sb_steps,
                         &c.scan_tmp, &c.dense_arena, &c.dense_meta, &c.dense_out, &c.spectra, &c.th_beta,
                         &c.th_mu, &c.th_state, &c.hl_ptr, &c.hl_ent};
   for (auto* b : bufs) b->release();
@@ -227,6 +229,42 @@ int ftlm_blocks_exact_batched(ftlm_ctx* ctx, const int32_t* mx, const int32_t* m
       list.emplace_back(mx[i], my[i]);
     }
     ftlm::run_exact_blocks(c, list);
+  });
+}
+
+int ftlm_blocks_ftlm_batched(ftlm_ctx* ctx, const int32_t* mx, const int32_t* my, int32_t nblocks) {
+  return ftlm::guarded(ctx, [&](Ctx& c) {
+    ftlm::need_sector(c);
+    if (nblocks < 0 || (nblocks > 0 && (!mx || !my))) throw Error(FTLM_ERR_ARG, "bad block list");
+    static_assert(FTLM_SMALL_BLOCK_MAX == ftlm::kSmallMaxDim, "small-block limit");
+    std::vector<std::pair<int, int>> small, large;
+    for (int i = 0; i < nblocks; ++i) {
+      ftlm::check_k(c, mx[i], my[i]);
+      const int64_t d = ftlm::block_dim_only(c, mx[i], my[i]);
+      if (d <= 0) continue;
+      (c.small_blocks && d <= ftlm::kSmallMaxDim ? small : large).emplace_back(mx[i], my[i]);
+    }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (c.timing) {
+      FTLM_CUDA(cudaEventCreate(&e0));
+      FTLM_CUDA(cudaEventCreate(&e1));
+      FTLM_CUDA(cudaEventRecord(e0, c.stream));
+    }
+    ftlm::run_small_ftlm_blocks(c, small);
+    for (const auto& b : large) {
+      ftlm::Spectrum s;
+      ftlm::run_ftlm_block(c, c.sec.n_up, c.sec.n_dn, b.first, b.second, s, nullptr, nullptr, nullptr, nullptr);
+      c.spec[b] = s;
+    }
+    if (c.timing) {
+      FTLM_CUDA(cudaEventRecord(e1, c.stream));
+      FTLM_CUDA(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      FTLM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      c.prof.block_ms += ms;
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+    }
   });
 }
 
@@ -480,6 +518,8 @@ int ftlm_profile_read(ftlm_ctx* ctx, ftlm_profile* out) {
     out->d2h_bytes = p.d2h_bytes;
     out->hv_variant = p.hv_variant;
     out->tune_runs = p.tune_runs;
+    out->small_ms = p.small_ms;
+    out->small_tasks = p.small_tasks;
   });
 }
 

@@ -190,6 +190,25 @@ __device__ __host__ __forceinline__ P4 philox4x32_10(P4 c, uint32_t k0, uint32_t
   return c;
 }
 
+// Production start-vector element: unit-modulus phase exp(2 pi i u) * amp,
+// u uniform in [0, 1) from Philox keyed by the block seed with counter
+// (row, sample).
+__device__ __forceinline__ void philox_phase(int64_t row, int sample, uint64_t seed, double amp, double& re,
+                                             double& im) {
+  P4 ctr;
+  ctr.x[0] = static_cast<uint32_t>(row);
+  ctr.x[1] = static_cast<uint32_t>(static_cast<uint64_t>(row) >> 32);
+  ctr.x[2] = static_cast<uint32_t>(sample);
+  ctr.x[3] = 0x46544C4Du;
+  const P4 r = philox4x32_10(ctr, static_cast<uint32_t>(seed), static_cast<uint32_t>(seed >> 32));
+  const uint64_t bits53 = (static_cast<uint64_t>(r.x[0]) << 21) ^ (r.x[1] >> 11);
+  const double u = static_cast<double>(bits53 & ((1ULL << 53) - 1)) * (1.0 / 9007199254740992.0);
+  double sn, cs;
+  sincospi(2.0 * u, &sn, &cs);
+  re = amp * cs;
+  im = amp * sn;
+}
+
 // Packed lookup entries.
 //  up_info: ur(32) | g0(8)<<32 | sign(1)<<40   (T_g0 maps the up
 //           representative onto this up word with that sign)

@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <map>
 #include <stdexcept>
@@ -40,6 +41,20 @@ struct DBuf {
     if (bytes == 0) return;
     FTLM_CUDA(cudaMalloc(&p, bytes));
     cap = bytes;
+  }
+  // Grows (by at least half) keeping the first `cap` bytes; stream-ordered copy.
+  void ensure_keep(size_t bytes, cudaStream_t stream) {
+    if (bytes <= cap) return;
+    const size_t want = std::max(bytes, cap + cap / 2);
+    void* q = nullptr;
+    FTLM_CUDA(cudaMalloc(&q, want));
+    if (p) {
+      FTLM_CUDA(cudaMemcpyAsync(q, p, cap, cudaMemcpyDeviceToDevice, stream));
+      FTLM_CUDA(cudaStreamSynchronize(stream));
+      FTLM_CUDA(cudaFree(p));
+    }
+    p = q;
+    cap = want;
   }
   template <typename T>
   T* as() const { return static_cast<T*>(p); }
@@ -138,7 +153,13 @@ struct Profile {
   int64_t h2d_bytes = 0, d2h_bytes = 0;
   int hv_variant = -1;  // H*V kernel variant of the last launch
   int tune_runs = 0;    // autotuner measurements made by this context
+  double small_ms = 0.0;     // device time of small-block Lanczos launches
+  int64_t small_tasks = 0;   // (block, random vector) pairs they ran
 };
+
+// Largest block dimension the small-block Lanczos launch takes (three FP64
+// complex vectors of this length fill 192 KB of shared memory).
+constexpr int64_t kSmallMaxDim = 4096;
 
 struct Ctx {
   ftlm_model model{};
@@ -148,6 +169,7 @@ struct Ctx {
   int hv_forced = -1; // H*V kernel variant forced by FTLM_HV_VARIANT (-1: autotune)
   int hv_mode = -1;   // H*V operator source: -1 auto, 0 on-the-fly lookups, 1 cached hop list (FTLM_HV_MODE)
   bool hl_active = false;  // H*V kernels read the cached hop list of the prepared block
+  bool small_blocks = true;  // batched FTLM runs blocks <= kSmallMaxDim in one launch (FTLM_SMALL_BLOCKS=0: off)
   int64_t hl_nnz = 0;
   DBuf hl_ptr, hl_ent;     // hop list: int64 row pointers, packed uint64 entries
   int device = 0;
@@ -160,9 +182,11 @@ struct Ctx {
   BlockTables blk;
   // Lanczos work space
   DBuf vec_a, vec_b, vec_h, partial, lz_alpha, lz_beta, lz_scale, lz_state, host_start;
-  DBuf ritz_tmp, scan_tmp;
+  DBuf ritz_tmp, ritz_out, scan_tmp;
   // exact batch
   DBuf dense_arena, dense_meta, dense_out;
+  // small-block FTLM batch: CSR arenas, task list, per-vector step counts
+  DBuf sb_rp, sb_col, sb_val, sb_diag, sb_meta, sb_steps;
   // spectra of the current sector's blocks (device arena)
   DBuf spectra;
   int64_t spectra_used = 0;
@@ -200,6 +224,13 @@ void run_ftlm_block(Ctx& c, int n_up, int n_dn, int mx, int my, Spectrum& out,
                     const double* host_start /* [R][dim] complex or null */,
                     std::vector<double>* alpha_out, std::vector<double>* beta_out,
                     std::vector<int32_t>* steps_out);
+// FTLM spectra of several small blocks (dim <= kSmallMaxDim) of the prepared
+// sector in one persistent launch; stored like run_ftlm_block's.
+void run_small_ftlm_blocks(Ctx& c, const std::vector<std::pair<int, int>>& blocks);
+// Ritz values and weights of R Lanczos runs (alpha/beta [sweep][K][ld],
+// nvmax vectors per sweep, steps[R] on the device) into the spectra arena.
+void ritz_stage(Ctx& c, int R, int nvmax, int ld, int K, const double* alpha, const double* beta,
+                const int32_t* steps, Spectrum& out);
 // Exact spectra of several blocks of the prepared sector (one batched launch).
 void run_exact_blocks(Ctx& c, const std::vector<std::pair<int, int>>& blocks);
 // Thermo

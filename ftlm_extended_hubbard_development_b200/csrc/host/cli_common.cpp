@@ -580,6 +580,19 @@ int run_ftlm_main(int argc, char** argv) {  // main.cpp:1459-1839
           }
         eng.check(ftlm_blocks_exact_batched(eng.ctx(), ex_mx.data(), ex_my.data(), static_cast<int>(ex_mx.size())),
                   "blocks_exact_batched");
+        // and every FTLM spectrum of blocks without exact/trace/debug output
+        std::vector<int32_t> ft_mx, ft_my;
+        for (int my = 0; my < params.ly; ++my)
+          for (int mx = 0; mx < params.lx; ++mx) {
+            const uint64_t dim = info.block_dim[my * params.lx + mx];
+            if (dim == 0 || dim <= params.exact_block_threshold || ckpt.count(BlockKey{n_up, n_down, mx, my}) ||
+                trace_blocks || matches(mx, my))
+              continue;
+            ft_mx.push_back(mx);
+            ft_my.push_back(my);
+          }
+        eng.check(ftlm_blocks_ftlm_batched(eng.ctx(), ft_mx.data(), ft_my.data(), static_cast<int>(ft_mx.size())),
+                  "blocks_ftlm_batched");
         std::size_t active_sum = 0;
         for (int my = 0; my < params.ly; ++my) {
           for (int mx = 0; mx < params.lx; ++mx) {

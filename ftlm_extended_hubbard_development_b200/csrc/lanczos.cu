@@ -163,20 +163,7 @@ __global__ void k_start_philox(int64_t dim, int NV, int nva, int sample0, uint64
       const int v = c * VPL + e;
       re[e] = 0.0;
       im[e] = 0.0;
-      if (v < nva) {
-        P4 ctr;
-        ctr.x[0] = static_cast<uint32_t>(row);
-        ctr.x[1] = static_cast<uint32_t>(static_cast<uint64_t>(row) >> 32);
-        ctr.x[2] = static_cast<uint32_t>(sample0 + v);
-        ctr.x[3] = 0x46544C4Du;
-        const P4 r = philox4x32_10(ctr, static_cast<uint32_t>(seed), static_cast<uint32_t>(seed >> 32));
-        const uint64_t bits53 = (static_cast<uint64_t>(r.x[0]) << 21) ^ (r.x[1] >> 11);
-        const double u = static_cast<double>(bits53 & ((1ULL << 53) - 1)) * (1.0 / 9007199254740992.0);
-        double sn, cs;
-        sincospi(2.0 * u, &sn, &cs);
-        re[e] = amp * cs;
-        im[e] = amp * sn;
-      }
+      if (v < nva) philox_phase(row, sample0 + v, seed, amp, re[e], im[e]);
     }
     V o;
     if constexpr (VPL == 2) {
@@ -436,6 +423,53 @@ void spectra_reset(Ctx& c) {
   c.spec.clear();
 }
 
+void ritz_stage(Ctx& c, int R, int nvmax, int ld, int K, const double* alpha, const double* beta,
+                const int32_t* steps, Spectrum& out) {
+  const int64_t off = spectra_alloc(c, 2 * static_cast<int64_t>(R) * K);
+  c.ritz_out.ensure(sizeof(double) * 3 * static_cast<size_t>(R) * K + 64);
+  double* dtmp = c.ritz_out.as<double>();
+  double* ztmp = dtmp + static_cast<size_t>(R) * K;
+  double* etmp = ztmp + static_cast<size_t>(R) * K;
+  int* status = reinterpret_cast<int*>(etmp + static_cast<size_t>(R) * K);
+  int64_t* total = reinterpret_cast<int64_t*>(status + 2);
+  FTLM_CUDA(cudaMemsetAsync(status, 0, sizeof(int), c.stream));
+  cudaEvent_t ee0 = nullptr, ee1 = nullptr;
+  if (c.timing) {
+    FTLM_CUDA(cudaEventCreate(&ee0));
+    FTLM_CUDA(cudaEventCreate(&ee1));
+    FTLM_CUDA(cudaEventRecord(ee0, c.stream));
+  }
+  const size_t tsmem = sizeof(double) * 3 * 32 * static_cast<size_t>(K);
+  const int use_smem = tsmem <= 200 * 1024;
+  if (use_smem && tsmem > 48 * 1024)
+    FTLM_CUDA(cudaFuncSetAttribute(k_tridiag, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(tsmem)));
+  k_tridiag<<<(R + 31) / 32, 32, use_smem ? tsmem : 0, c.stream>>>(R, nvmax, ld, K, alpha, beta, steps, dtmp, ztmp,
+                                                                  etmp, 1.0 / R, status, use_smem);
+  if (c.timing) FTLM_CUDA(cudaEventRecord(ee1, c.stream));
+  k_compact<<<1, 256, sizeof(int) * (R + 1), c.stream>>>(R, K, steps, dtmp, ztmp, c.spectra.as<double>() + off,
+                                                          c.spectra.as<double>() + off + static_cast<int64_t>(R) * K,
+                                                          total);
+  FTLM_LAUNCH_CHECK();
+  c.prof.kernel_launches += 2;
+  int64_t cnt = 0;
+  int hstatus = 0;
+  FTLM_CUDA(cudaMemcpyAsync(&cnt, total, sizeof(int64_t), cudaMemcpyDeviceToHost, c.stream));
+  FTLM_CUDA(cudaMemcpyAsync(&hstatus, status, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  FTLM_CUDA(cudaStreamSynchronize(c.stream));
+  if (hstatus) throw Error(FTLM_ERR_NUMERIC, "tridiagonal QL did not converge");
+  if (c.timing) {
+    float ms = 0.f;
+    FTLM_CUDA(cudaEventElapsedTime(&ms, ee0, ee1));
+    c.prof.eig_ms += ms;
+    cudaEventDestroy(ee0);
+    cudaEventDestroy(ee1);
+  }
+  out.ev_off = off;
+  out.w_off = off + static_cast<int64_t>(R) * K;
+  out.count = cnt;
+  out.exact = false;
+}
+
 void run_ftlm_block(Ctx& c, int n_up, int n_dn, int mx, int my, Spectrum& out, const double* host_start,
                     std::vector<double>* alpha_out, std::vector<double>* beta_out, std::vector<int32_t>* steps_out) {
   block_prepare(c, mx, my);
@@ -447,7 +481,6 @@ void run_ftlm_block(Ctx& c, int n_up, int n_dn, int mx, int my, Spectrum& out, c
   int nvmax = c.opts.batch_vectors > 0 ? c.opts.batch_vectors : std::min(R, 128);
   nvmax = std::min(nvmax, 128);
   const uint64_t bseed = block_seed(c.opts.seed, n_up, n_dn, mx, my);
-  const int64_t off = spectra_alloc(c, 2 * static_cast<int64_t>(R) * K);
   if (alpha_out) {
     alpha_out->assign(static_cast<size_t>(R) * c.opts.lanczos_steps, 0.0);
     beta_out->assign(static_cast<size_t>(R) * c.opts.lanczos_steps, 0.0);
@@ -459,14 +492,8 @@ void run_ftlm_block(Ctx& c, int n_up, int n_dn, int mx, int my, Spectrum& out, c
   c.lz_alpha.ensure(sizeof(double) * static_cast<size_t>(nsweep) * K * ld);
   c.lz_beta.ensure(sizeof(double) * static_cast<size_t>(nsweep) * K * ld);
   FTLM_CUDA(cudaMemsetAsync(c.lz_beta.p, 0, sizeof(double) * static_cast<size_t>(nsweep) * K * ld, c.stream));
-  c.ritz_tmp.ensure(sizeof(double) * 3 * static_cast<size_t>(R) * K + sizeof(int32_t) * (R + 8) + 64);
-  double* dtmp = c.ritz_tmp.as<double>();
-  double* ztmp = dtmp + static_cast<size_t>(R) * K;
-  double* etmp = ztmp + static_cast<size_t>(R) * K;
-  int32_t* steps_all = reinterpret_cast<int32_t*>(etmp + static_cast<size_t>(R) * K);
-  int* status = steps_all + R;
-  int64_t* total = reinterpret_cast<int64_t*>(reinterpret_cast<uintptr_t>(status + 2 + 7) & ~uintptr_t(7));
-  FTLM_CUDA(cudaMemsetAsync(status, 0, sizeof(int), c.stream));
+  c.ritz_tmp.ensure(sizeof(int32_t) * (R + 8));
+  int32_t* steps_all = c.ritz_tmp.as<int32_t>();
   std::vector<double> hstart;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> evs;
   double hv_bytes = 0.0;
@@ -565,29 +592,7 @@ void run_ftlm_block(Ctx& c, int n_up, int n_dn, int mx, int my, Spectrum& out, c
     c.last_nv = NV;
   }
   // Ritz values and weights of all sweeps in one batched launch
-  cudaEvent_t ee0 = nullptr, ee1 = nullptr;
-  if (c.timing) {
-    FTLM_CUDA(cudaEventCreate(&ee0));
-    FTLM_CUDA(cudaEventCreate(&ee1));
-    FTLM_CUDA(cudaEventRecord(ee0, c.stream));
-  }
-  const size_t tsmem = sizeof(double) * 3 * 32 * static_cast<size_t>(K);
-  const int use_smem = tsmem <= 200 * 1024;
-  if (use_smem && tsmem > 48 * 1024)
-    FTLM_CUDA(cudaFuncSetAttribute(k_tridiag, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(tsmem)));
-  k_tridiag<<<(R + 31) / 32, 32, use_smem ? tsmem : 0, c.stream>>>(R, nvmax, ld, K, c.lz_alpha.as<double>(),
-                                                                  c.lz_beta.as<double>(), steps_all, dtmp, ztmp, etmp,
-                                                                  1.0 / R, status, use_smem);
-  if (c.timing) FTLM_CUDA(cudaEventRecord(ee1, c.stream));
-  k_compact<<<1, 256, sizeof(int) * (R + 1), c.stream>>>(R, K, steps_all, dtmp, ztmp, c.spectra.as<double>() + off,
-                                                          c.spectra.as<double>() + off + static_cast<int64_t>(R) * K,
-                                                          total);
-  FTLM_LAUNCH_CHECK();
-  c.prof.kernel_launches += 2;
-  int64_t cnt = 0;
-  int hstatus = 0;
-  FTLM_CUDA(cudaMemcpyAsync(&cnt, total, sizeof(int64_t), cudaMemcpyDeviceToHost, c.stream));
-  FTLM_CUDA(cudaMemcpyAsync(&hstatus, status, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  ritz_stage(c, R, nvmax, ld, K, c.lz_alpha.as<double>(), c.lz_beta.as<double>(), steps_all, out);
   if (alpha_out) {
     std::vector<double> a(static_cast<size_t>(nsweep) * K * ld), b(a.size());
     std::vector<int32_t> sv(R);
@@ -604,8 +609,6 @@ void run_ftlm_block(Ctx& c, int n_up, int n_dn, int mx, int my, Spectrum& out, c
       for (int j = 0; j + 1 < n; ++j) (*beta_out)[static_cast<size_t>(r) * L + j] = b[base + static_cast<size_t>(j) * ld];
     }
   }
-  FTLM_CUDA(cudaStreamSynchronize(c.stream));
-  if (hstatus) throw Error(FTLM_ERR_NUMERIC, "tridiagonal QL did not converge");
   if (c.timing) {
     for (auto& pr : evs) {
       float ms = 0.f;
@@ -615,17 +618,8 @@ void run_ftlm_block(Ctx& c, int n_up, int n_dn, int mx, int my, Spectrum& out, c
       cudaEventDestroy(pr.first);
       cudaEventDestroy(pr.second);
     }
-    float ms = 0.f;
-    FTLM_CUDA(cudaEventElapsedTime(&ms, ee0, ee1));
-    c.prof.eig_ms += ms;
-    cudaEventDestroy(ee0);
-    cudaEventDestroy(ee1);
     c.prof.hv_bytes += hv_bytes;
   }
-  out.ev_off = off;
-  out.w_off = off + static_cast<int64_t>(R) * K;
-  out.count = cnt;
-  out.exact = false;
   out.prefactor = static_cast<double>(D);
   out.particles = n_up + n_dn;
   out.dim = D;

@@ -56,12 +56,14 @@ class _Profile(C.Structure):
                 ("eig_ms", C.c_double), ("dense_ms", C.c_double), ("thermo_ms", C.c_double),
                 ("sector_ms", C.c_double), ("block_ms", C.c_double),
                 ("kernel_launches", C.c_int64), ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64),
-                ("hv_variant", C.c_int32), ("tune_runs", C.c_int32)]
+                ("hv_variant", C.c_int32), ("tune_runs", C.c_int32), ("small_ms", C.c_double),
+                ("small_tasks", C.c_int64)]
 
 
 EXPORTS = [
     "ftlm_abi_version", "ftlm_ctx_create", "ftlm_ctx_destroy", "ftlm_last_error",
     "ftlm_sector_prepare", "ftlm_block_spectrum", "ftlm_spectra_reset", "ftlm_blocks_exact_batched",
+    "ftlm_blocks_ftlm_batched",
     "ftlm_thermo_configure", "ftlm_thermo_accumulate_block", "ftlm_thermo_accumulate_host",
     "ftlm_thermo_read", "ftlm_block_apply", "ftlm_block_lanczos",
     "ftlm_debug_sector_parents", "ftlm_debug_sector_relations", "ftlm_debug_block_csr",
@@ -92,6 +94,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "ftlm_block_spectrum": ([vp, i32, i32, i32, vp, vp, sz, P(sz), P(d)], C.c_int),
         "ftlm_spectra_reset": ([vp], C.c_int),
         "ftlm_blocks_exact_batched": ([vp, vp, vp, i32], C.c_int),
+        "ftlm_blocks_ftlm_batched": ([vp, vp, vp, i32], C.c_int),
         "ftlm_thermo_configure": ([vp, i32, vp, i32, vp], C.c_int),
         "ftlm_thermo_accumulate_block": ([vp, i32, i32], C.c_int),
         "ftlm_thermo_accumulate_host": ([vp, vp, vp, sz, d, i32], C.c_int),
@@ -234,6 +237,12 @@ class Engine:
         my = np.array([b[1] for b in blocks], np.int32)
         self._check(self.lib.ftlm_blocks_exact_batched(self.h, _p(mx), _p(my), len(blocks)))
 
+    def blocks_ftlm_batched(self, blocks):
+        """FTLM spectra of several blocks; the small ones in one persistent launch."""
+        mx = np.array([b[0] for b in blocks], np.int32)
+        my = np.array([b[1] for b in blocks], np.int32)
+        self._check(self.lib.ftlm_blocks_ftlm_batched(self.h, _p(mx), _p(my), len(blocks)))
+
     # ---- thermodynamics
     def thermo_configure(self, betas, mu):
         self._betas = np.ascontiguousarray(betas, np.float64)
@@ -344,9 +353,8 @@ def run_curve(model: Model, betas, mu, opts: RunOpts | None = None, ed: bool = F
                 exact = [b for b in blocks
                          if ed or info.block_dims[b[1] * model.lx + b[0]] <= opts.exact_block_threshold]
                 eng.blocks_exact_batched(exact)
+                eng.blocks_ftlm_batched([b for b in blocks if b not in exact])
                 for b in blocks:
-                    if b not in exact:
-                        eng.block_spectrum(b[0], b[1], exact=False, fetch=False)
                     eng.thermo_accumulate_block(*b)
         emin, z, ns, n2 = eng.thermo_read()
     finally:

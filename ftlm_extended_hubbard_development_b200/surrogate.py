@@ -1,9 +1,9 @@
 """Learned twist surrogate: per-block low-lying spectra as a function of twist.
 
-A small FP32 MLP (engine.Mlp, trained on the GPU by the library's own
-forward / backward / Adam kernels) maps a block's twist and quantum numbers
+Small FP32 MLPs (engine.Mlp, trained on the GPU by the library's own forward /
+backward / Adam kernels) map a block's twist and quantum numbers
 (phi_x, phi_y, N_up, N_down, k_x, k_y) to the block's `levels` lowest energy
-levels and their trace weights. Its training data are the spectra the GPU
+levels and their trace weights. The training data are the spectra the GPU
 engine itself produces on a uniform grid of twists. From the predicted levels
 the surrogate proposes the n(mu) curve at any twist, e.g. on a dense grid for
 the twist average. Plain FTLM (or ED) at held-out twists is its judge: when
@@ -11,22 +11,32 @@ the surrogate's n(mu) there is off by more than the threshold, the twist
 average falls back to the engine's own twists.
 
 Per block and twist the spectrum is split in two:
-  * low part - the block spectrum sorted and merged into levels (Ritz values
-    of different random vectors that agree to `tol`, and degenerate
-    eigenvalues), each with its total trace weight (prefactor * summed FTLM
-    weights, or the multiplicity for an exact block); the lowest `levels` of
-    them are the network's targets, masked where the block has fewer;
+  * low part - the lowest `levels` levels: for an exactly diagonalised block
+    its lowest eigenvalues one by one (weight 1 each); for an FTLM block the
+    Ritz values merged across random vectors where they agree to `tol`, each
+    with its summed trace weight (prefactor * FTLM weights). These are the
+    network's targets, masked where the block has fewer levels;
   * tail - everything above, kept only as its partition sum per beta,
     log sum_i w_i exp(-beta e_i).
 A proposal at twist phi takes the low part from the network and the tail of
-the training twist nearest to phi, so truncating the spectrum costs nothing
-at the training twists and little elsewhere. The network learns the twist
-dependence on top of a per-(block, level) mean over the training twists, so
-its output is a small correction with unit-scaled targets.
+the training twist nearest to phi; the tail's Boltzmann weight is small, so
+truncating the spectrum costs little.
 
-A block's spectrum is not periodic with period 1 in phi: the gauge change
-that removes one flux quantum moves the block to momentum k + N. The inputs
-therefore carry the per-bond phase 2 pi phi / L beside 2 pi phi.
+Inputs. A block's spectrum has period L in its own twist (the per-bond phase
+is 2 pi phi / L) but not period 1: the gauge change that removes one flux
+quantum moves the block to momentum k + N. The twist enters as sin/cos of the
+per-bond phase and of its second harmonic; the quantum numbers enter one-hot,
+which lets one network keep the blocks apart.
+
+Targets and loss. The network predicts the deviation from the per-(block,
+level) mean over the training twists, in units of the global spread of those
+deviations. Each target is weighted by its importance for n(mu): the largest
+Boltzmann probability the level reaches on the (beta, mu) grid, plus 1e-3, so
+the network's capacity goes to the levels that set the curve.
+
+Training: Adam, mini-batches of 512 (block, twist) rows, learning rate stepped
+down over six stages; an ensemble of `members` networks (different seeds)
+whose mean is the prediction.
 """
 from __future__ import annotations
 
@@ -39,23 +49,38 @@ from .engine import Engine, Mlp, Model, RunOpts
 from .twist import combine_rows, curve_rows, uniform_grid
 
 LEVELS = 16
-N_FEAT = 14
+HARMONICS = 2
+MEMBERS = 3
+# learning-rate factors of the six training stages (a stepped cosine decay)
+LR_STAGES = (1.0, 0.8, 0.55, 0.3, 0.12, 0.03)
+
+
+def n_features(model: Model) -> int:
+    return 4 * HARMONICS + 2 * (model.sites + 1) + model.lx + model.ly
 
 
 def block_features(phix, phiy, nup, ndn, mx, my, lx, ly):
-    """Network input of one block at one twist: periodic quantities as
-    sin/cos pairs, particle numbers as fillings."""
+    """Network input of one block at one twist: sin/cos of the per-bond twist
+    phase and its harmonics, then one-hot N_up, N_down, k_x, k_y."""
     t = 2.0 * math.pi
     n = lx * ly
-    return [math.sin(t * phix), math.cos(t * phix), math.sin(t * phiy), math.cos(t * phiy),
-            math.sin(t * phix / lx), math.cos(t * phix / lx), math.sin(t * phiy / ly), math.cos(t * phiy / ly),
-            nup / n, ndn / n, math.cos(t * mx / lx), math.sin(t * mx / lx), math.cos(t * my / ly),
-            math.sin(t * my / ly)]
+    f = []
+    for h in range(1, HARMONICS + 1):
+        f += [math.sin(h * t * phix / lx), math.cos(h * t * phix / lx), math.sin(h * t * phiy / ly),
+              math.cos(h * t * phiy / ly)]
+    oh = [0.0] * (2 * (n + 1) + lx + ly)
+    oh[nup] = 1.0
+    oh[n + 1 + ndn] = 1.0
+    oh[2 * (n + 1) + mx] = 1.0
+    oh[2 * (n + 1) + lx + my] = 1.0
+    return f + oh
 
 
 def reduce_spectrum(ev, w, pref, exact, levels=LEVELS, tol=1e-6):
-    """Lowest `levels` merged levels (energy, trace weight, present mask) of a
-    block, and the remaining (energies, trace weights) as the tail."""
+    """Lowest `levels` levels (energy, trace weight, present mask) of a block
+    and the remaining (energies, trace weights) as the tail. Exact blocks keep
+    every eigenvalue as its own level (weight 1); FTLM Ritz values that agree
+    to `tol` (relative) are merged and their weights summed."""
     ev = np.asarray(ev, np.float64)
     o = np.argsort(ev, kind="stable")
     e = ev[o]
@@ -66,7 +91,7 @@ def reduce_spectrum(ev, w, pref, exact, levels=LEVELS, tol=1e-6):
     k = -1
     cut = len(e)
     for i in range(len(e)):
-        if k >= 0 and abs(e[i] - E[k]) <= tol * max(1.0, abs(E[k])):
+        if not exact and k >= 0 and abs(e[i] - E[k]) <= tol * max(1.0, abs(E[k])):
             W[k] += ww[i]
             continue
         if k + 1 >= levels:
@@ -93,8 +118,8 @@ def tail_log_partition(e, w, betas):
 @dataclass
 class TwistData:
     """Engine output at one twist: per block (nup, ndn, mx, my, particles,
-    E[levels], W[levels], M[levels], tail_logz[nbeta]) and the engine's own
-    n(mu) curve (dict of [nbeta][nmu] arrays)."""
+    E[levels], W[levels], M[levels], tail_logz[nbeta], exact) and the
+    engine's own n(mu) curve (dict of [nbeta][nmu] arrays)."""
     phix: float
     phiy: float
     blocks: list
@@ -116,11 +141,13 @@ def collect(model: Model, phix, phiy, betas, mu, opts: RunOpts, ed=False, levels
                 exact = [b for b in ks
                          if ed or info.block_dims[b[1] * model.lx + b[0]] <= opts.exact_block_threshold]
                 eng.blocks_exact_batched(exact)
+                eng.blocks_ftlm_batched([b for b in ks if b not in exact])
                 for b in ks:
                     is_exact = b in exact
                     ev, w, pref = eng.block_spectrum(b[0], b[1], exact=is_exact)
                     E, W, M, te, tw = reduce_spectrum(ev, w, pref, is_exact, levels)
-                    blocks.append((nu, nd, b[0], b[1], nu + nd, E, W, M, tail_log_partition(te, tw, betas)))
+                    blocks.append((nu, nd, b[0], b[1], nu + nd, E, W, M, tail_log_partition(te, tw, betas),
+                                   is_exact))
                     eng.thermo_accumulate_block(*b)
         emin, z, ns, n2 = eng.thermo_read()
     finally:
@@ -133,29 +160,39 @@ def collect(model: Model, phix, phiy, betas, mu, opts: RunOpts, ed=False, levels
     return TwistData(float(phix), float(phiy), blocks, curve)
 
 
+def _shift(blocks, mu):
+    shift = np.full(len(mu), np.inf)
+    for b in blocks:
+        if b[7].any():
+            shift = np.minimum(shift, b[5][b[7] > 0].min() - mu * b[4])
+    return shift
+
+
+def _block_z(b, beta, mu, shift, ib):
+    sel = b[7] > 0
+    zz = (b[6][sel, None] * np.exp(-beta * (b[5][sel, None] - mu[None, :] * b[4] - shift[None, :]))).sum(0)
+    if np.isfinite(b[8][ib]):
+        zz = zz + np.exp(b[8][ib] + beta * (mu * b[4] + shift))
+    return zz
+
+
 def curve_from_blocks(blocks, sites, betas, mu):
     """n(mu) observables from per-block levels plus tail partition sums; the
     shifted log-sum-exp of the reference (main.cpp:1172-1219, 1770-1788)
     with one shift per mu, the lowest level of any block minus mu * N."""
     mu = np.asarray(mu, np.float64)
-    shift = np.full(len(mu), np.inf)
-    for b in blocks:
-        if b[7].any():
-            shift = np.minimum(shift, b[5][b[7] > 0].min() - mu * b[4])
+    shift = _shift(blocks, mu)
     out = {k: np.zeros((len(betas), len(mu))) for k in
            ("n", "charge_correlation", "compressibility", "partition_like", "log_partition")}
     for ib, beta in enumerate(betas):
         z = np.zeros(len(mu))
         n1 = np.zeros(len(mu))
         n2 = np.zeros(len(mu))
-        for nu, nd, mx, my, p, E, W, M, tail in blocks:
-            sel = M > 0
-            zz = (W[sel, None] * np.exp(-beta * (E[sel, None] - mu[None, :] * p - shift[None, :]))).sum(0)
-            if np.isfinite(tail[ib]):
-                zz = zz + np.exp(tail[ib] + beta * (mu * p + shift))
+        for b in blocks:
+            zz = _block_z(b, beta, mu, shift, ib)
             z += zz
-            n1 += p * zz
-            n2 += p * p * zz
+            n1 += b[4] * zz
+            n2 += b[4] * b[4] * zz
         mean = n1 / z
         chi = np.maximum(0.0, (n2 / z - mean * mean) / sites)
         out["n"][ib] = mean / sites
@@ -166,6 +203,20 @@ def curve_from_blocks(blocks, sites, betas, mu):
     return out
 
 
+def level_importance(blocks, betas, mu):
+    """Largest Boltzmann probability each level reaches on the (beta, mu)
+    grid: [nblocks][levels]."""
+    mu = np.asarray(mu, np.float64)
+    shift = _shift(blocks, mu)
+    imp = np.zeros((len(blocks), len(blocks[0][5])))
+    for ib, beta in enumerate(betas):
+        z = sum(_block_z(b, beta, mu, shift, ib) for b in blocks)
+        for i, b in enumerate(blocks):
+            p = b[6][:, None] * np.exp(-beta * (b[5][:, None] - mu[None, :] * b[4] - shift[None, :])) / z[None, :]
+            imp[i] = np.maximum(imp[i], np.where(b[7] > 0, p.max(1), 0.0))
+    return imp
+
+
 def _dist2(a, b, wrap):
     d = [abs(x - y) for x, y in zip(a, b)]
     if wrap:
@@ -174,70 +225,70 @@ def _dist2(a, b, wrap):
 
 
 class TwistSurrogate:
-    """MLP over (twist, block quantum numbers) -> lowest levels and weights."""
+    """Ensemble of MLPs over (twist, block quantum numbers) -> lowest levels
+    and weights of every block."""
 
-    def __init__(self, model: Model, levels=LEVELS, width=128, depth=3, seed=1234, device=0):
+    def __init__(self, model: Model, levels=LEVELS, width=128, depth=3, members=MEMBERS, seed=1234, device=0):
         self.model = model
         self.levels = levels
-        self.net = Mlp(N_FEAT, width, depth, 2 * levels, seed=seed, device=device)
+        self.nets = [Mlp(n_features(model), width, depth, 2 * levels, seed=seed + 7919 * i, device=device)
+                     for i in range(members)]
         self.keys = None
         self.train_data = None
 
     def close(self):
-        self.net.close()
-
-    def _tables(self, data):
-        keys = [b[:5] for b in data[0].blocks]
-        idx = {k: i for i, k in enumerate(keys)}
-        L = self.levels
-        E = np.zeros((len(data), len(keys), L))
-        W = np.zeros_like(E)
-        M = np.zeros_like(E)
-        for t, td in enumerate(data):
-            for b in td.blocks:
-                i = idx[b[:5]]
-                E[t, i], W[t, i], M[t, i] = b[5], b[6], b[7]
-        return keys, E, W, M
+        for n in self.nets:
+            n.close()
 
     def features(self, phix, phiy):
         lx, ly = self.model.lx, self.model.ly
         return np.array([block_features(phix, phiy, k[0], k[1], k[2], k[3], lx, ly) for k in self.keys],
                         np.float32)
 
-    def fit(self, data, epochs=1500, batch=512, lr=1e-3, seed=7):
+    def fit(self, data, betas, mu, epochs=600, batch=512, lr=1e-3, seed=7):
         """Train on the TwistData of the training twists; returns the loss
-        history (one value per epoch, Adam at lr, then a third as many epochs
-        at lr / 5)."""
+        history of the first member (one value per epoch)."""
         self.train_data = data
-        self.keys, E, W, M = self._tables(data)
-        mcount = np.maximum(M.sum(0), 1.0)
+        self.keys = [b[:5] for b in data[0].blocks]
+        self.exact = np.array([b[9] for b in data[0].blocks], bool)
+        L = self.levels
+        E = np.array([[b[5] for b in td.blocks] for td in data])
+        W = np.array([[b[6] for b in td.blocks] for td in data])
+        M = np.array([[b[7] for b in td.blocks] for td in data])
+        imp = np.array([level_importance(td.blocks, betas, mu) for td in data])
+        cnt = np.maximum(M.sum(0), 1.0)
         self.mask = (M.sum(0) > 0).astype(np.float64)  # a level present at any training twist
-        self.e0 = (E * M).sum(0) / mcount
-        self.w0 = (W * M).sum(0) / mcount
+        self.e0 = (E * M).sum(0) / cnt
+        self.w0 = (W * M).sum(0) / cnt
         rE = (E - self.e0) * M
         rW = (W - self.w0) * M
-        cnt = max(M.sum(), 1.0)
-        self.se = max(float(np.sqrt((rE ** 2).sum() / cnt)), 1e-6)
-        self.sw = max(float(np.sqrt((rW ** 2).sum() / cnt)), 1e-6)
+        fw = M * (~self.exact)[None, :, None]  # weights are learned for FTLM levels only
+        self.se = max(float(np.sqrt((rE ** 2).sum() / max(M.sum(), 1.0))), 1e-6)
+        self.sw = max(float(np.sqrt((rW ** 2 * fw).sum() / max(fw.sum(), 1.0))), 1e-6)
         X = np.concatenate([self.features(td.phix, td.phiy) for td in data])
-        T = np.concatenate([np.concatenate([rE[t] / self.se, rW[t] / self.sw], 1) for t in range(len(data))])
-        Mk = np.concatenate([np.concatenate([M[t], M[t]], 1) for t in range(len(data))])
-        T, Mk = T.astype(np.float32), Mk.astype(np.float32)
-        h1 = self.net.train(X, T, Mk, epochs, batch, lr, seed)
-        h2 = self.net.train(X, T, Mk, max(epochs // 3, 1), batch, lr / 5, seed + 1)
-        return np.concatenate([h1, h2])
+        T = np.concatenate([rE / self.se, rW / self.sw], 2).reshape(-1, 2 * L).astype(np.float32)
+        wgt = M * (1e-3 + imp)
+        Mk = np.concatenate([wgt, wgt * (~self.exact)[None, :, None]], 2).reshape(-1, 2 * L).astype(np.float32)
+        per = max(epochs // len(LR_STAGES), 1)
+        hist = []
+        for i, net in enumerate(self.nets):
+            h = [net.train(X, T, Mk, per, batch, lr * f, seed + 31 * i + s) for s, f in enumerate(LR_STAGES)]
+            if i == 0:
+                hist = np.concatenate(h)
+        return hist
 
     def nearest(self, phix, phiy, wrap=False):
         return min(self.train_data, key=lambda t: _dist2((t.phix, t.phiy), (phix, phiy), wrap))
 
     def predict_blocks(self, phix, phiy):
         """Blocks at a twist: predicted low levels, nearest training tail."""
-        y = self.net.forward(self.features(phix, phiy)).astype(np.float64)
+        x = self.features(phix, phiy)
+        y = sum(n.forward(x).astype(np.float64) for n in self.nets) / len(self.nets)
         L = self.levels
         E = self.e0 + y[:, :L] * self.se
-        W = np.maximum(self.w0 + y[:, L:] * self.sw, 0.0)
+        W = np.where(self.exact[:, None], 1.0, np.maximum(self.w0 + y[:, L:] * self.sw, 0.0))
         near = self.nearest(phix, phiy)
-        return [(*k, E[i], W[i], self.mask[i], near.blocks[i][8]) for i, k in enumerate(self.keys)]
+        return [(*k, E[i], W[i], self.mask[i], near.blocks[i][8], self.exact[i]) for i, k in enumerate(self.keys)]
 
     def curve(self, phix, phiy, betas, mu):
         return curve_from_blocks(self.predict_blocks(phix, phiy), self.model.sites, betas, mu)
@@ -250,15 +301,16 @@ def heldout_twists(count=8, seed=2024):
 
 
 def surrogate_twist_average(model: Model, betas, mu, opts: RunOpts, grid=6, heldout=8, dense=24,
-                            threshold=0.01, ed=False, epochs=1500, seed=2024, levels=LEVELS, device=0):
+                            threshold=0.01, ed=False, epochs=600, seed=2024, levels=LEVELS, members=MEMBERS,
+                            device=0):
     """Train on a grid x grid twist set, judge at `heldout` Philox twists with
     the engine, and average n(mu) over the surrogate's dense x dense grid when
     every judge passes (max |dn| <= threshold); otherwise average the
     engine's own curves at the training and held-out twists (fallback)."""
     opts = replace(opts, device=device)
     train = [collect(model, px, py, betas, mu, opts, ed, levels) for px, py in uniform_grid(grid)]
-    sur = TwistSurrogate(model, levels=levels, device=device)
-    hist = sur.fit(train, epochs=epochs)
+    sur = TwistSurrogate(model, levels=levels, members=members, device=device)
+    hist = sur.fit(train, betas, mu, epochs=epochs)
     judges = []
     for px, py in heldout_twists(heldout, seed):
         td = collect(model, px, py, betas, mu, opts, ed, levels)

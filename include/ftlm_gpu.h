@@ -82,6 +82,8 @@ typedef struct ftlm_profile {
   int64_t h2d_bytes, d2h_bytes;
   int32_t hv_variant;      /* H*V kernel variant used last (autotuned unless FTLM_HV_VARIANT is set) */
   int32_t tune_runs;       /* autotuner measurements made */
+  double small_ms;         /* small-block Lanczos launches (ftlm_blocks_ftlm_batched) */
+  int64_t small_tasks;     /* (block, random vector) pairs they ran */
 } ftlm_profile;
 
 typedef struct ftlm_ctx ftlm_ctx;
@@ -124,6 +126,17 @@ int ftlm_spectra_reset(ftlm_ctx* ctx);
  * device (diagonalize_block_exact, main.cpp:847-911, for a list of blocks). */
 int ftlm_blocks_exact_batched(ftlm_ctx* ctx, const int32_t* mx, const int32_t* my,
                               int32_t nblocks);
+
+/* FTLM spectra of several blocks of the prepared sector (run_ftlm_block,
+ * main.cpp:996-1113, for a list of blocks). Blocks of at most
+ * FTLM_SMALL_BLOCK_MAX rows run in one persistent launch, one CTA per
+ * (block, random vector) with the vectors in shared memory; larger blocks
+ * run one after another on the sweep path. Results stay on the device, as
+ * ftlm_block_spectrum(exact = 0) would leave them, and are what that call
+ * then returns. */
+#define FTLM_SMALL_BLOCK_MAX 4096
+int ftlm_blocks_ftlm_batched(ftlm_ctx* ctx, const int32_t* mx, const int32_t* my,
+                             int32_t nblocks);
 
 /* Grand-canonical accumulators over a beta list and mu grid (the
  * emin/z/n/n2 vectors of main.cpp:1500-1504 and 1748-1752). Resets them. */

@@ -60,13 +60,14 @@ def test_uniform_grid_and_heldout():
 def test_reduce_spectrum_merges_levels_and_splits_tail():
     ev = np.array([0.5, -1.0, -1.0 + 1e-9, 2.0, 0.5, 3.0, 4.0])
     w = np.array([0.1, 0.2, 0.3, 0.4, 0.5, 0.6, 0.7])
-    E, W, M, te, tw = reduce_spectrum(ev, w, 2.0, False, levels=3)
+    E, W, M, te, tw = reduce_spectrum(ev, w, 2.0, False, levels=3)  # FTLM: Ritz values merged
     assert np.allclose(E, [-1.0, 0.5, 2.0])
     assert np.allclose(W, [1.0, 1.2, 0.8])
     assert M.tolist() == [1, 1, 1]
     assert np.allclose(te, [3.0, 4.0]) and np.allclose(tw, [1.2, 1.4])
-    E, W, M, te, tw = reduce_spectrum(np.array([1.0, 1.0, 2.0]), None, 1.0, True, levels=4)
-    assert M.tolist() == [1, 1, 0, 0] and W.tolist()[:2] == [2.0, 1.0] and len(te) == 0
+    E, W, M, te, tw = reduce_spectrum(np.array([2.0, 1.0, 1.0]), None, 1.0, True, levels=4)  # exact: one by one
+    assert M.tolist() == [1, 1, 1, 0] and W.tolist() == [1, 1, 1, 0] and E.tolist()[:3] == [1, 1, 2]
+    assert len(te) == 0
 
 
 def test_curve_from_blocks_equals_direct_sums():
@@ -91,7 +92,11 @@ def test_curve_from_blocks_equals_direct_sums():
 
 
 def test_block_features_periodicity():
+    """Per-bond twist phases: period lx in phi_x, ly in phi_y, not 1."""
+    from ftlm_extended_hubbard_development_b200.surrogate import n_features
+    from ftlm_extended_hubbard_development_b200.engine import Model
     a = block_features(0.25, 0.5, 3, 4, 1, 0, 4, 2)
-    b = block_features(1.25, 0.5, 3, 4, 1, 0, 4, 2)
-    assert len(a) == 14
-    assert np.allclose(a[:4], b[:4]) and not np.allclose(a[4:6], b[4:6])
+    assert len(a) == n_features(Model(lx=4, ly=2)) == 32
+    assert np.allclose(a, block_features(4.25, 2.5, 3, 4, 1, 0, 4, 2))
+    assert not np.allclose(a, block_features(1.25, 0.5, 3, 4, 1, 0, 4, 2))
+    assert sum(a[8:]) == 4.0 and a[8 + 3] == 1 and a[8 + 9 + 4] == 1 and a[8 + 18 + 1] == 1 and a[8 + 22] == 1
