@@ -276,6 +276,107 @@ def run_ours(args):
         torch.distributed.destroy_process_group()
 
 
+# n(mu) curve workloads (--curve): model, betas, mu grid, samples x steps
+CURVES = {
+    "config2": dict(model=dict(lx=4, ly=2, tx=1.0, ty=1.0, tp=0.0, phix=1.0, phiy=1.0, u=8.0, v=0.0),
+                    betas=[20.0], mu=(-5.0, 15.0, 81), samples=32, steps=120, threshold=256,
+                    name="4x2 U=8 beta=20, 32 vectors x 120 steps, mu [-5,15] x 81"),
+    "config3": dict(model=dict(lx=4, ly=4, tx=1.0, ty=1.0, tp=0.0, phix=1.0, phiy=1.0, u=7.0, v=0.0),
+                    betas=[2.857142857142857, 12.5], mu=(-3.0, 4.0, 281), samples=128, steps=80, threshold=256,
+                    name="4x4 U=7 beta {2.857, 12.5}, 128 vectors x 80 steps, mu [-3,4] x 281"),
+}
+# The two GPU paths the curve metric compares. "plain": FP64 vectors, one
+# random vector per sweep, every block on the sweep kernels with on-the-fly
+# H*V; "batched": FP32 vectors with FP64 sums, all vectors of a block in one
+# sweep, small blocks in one persistent launch, hop list where it pays.
+PATHS = {
+    "mixed_batched": dict(precision="mixed", batch=0, env={"FTLM_SMALL_BLOCKS": "1", "FTLM_HV_MODE": "auto"}),
+    "fp64_batched": dict(precision="fp64", batch=0, env={"FTLM_SMALL_BLOCKS": "1", "FTLM_HV_MODE": "auto"}),
+    "fp64_plain": dict(precision="fp64", batch=1, env={"FTLM_SMALL_BLOCKS": "0", "FTLM_HV_MODE": "fly"}),
+}
+
+
+def time_curve(pkg, cfg, path, sectors=None, samples=None):
+    """Wall time of one n(mu) curve through the C ABI (block order of the
+    reference), or of the listed sectors only; returns (seconds, observables)."""
+    import numpy as np
+    p = PATHS[path]
+    os.environ.update(p["env"])
+    model = pkg.Model(**cfg["model"])
+    prec = pkg.engine.PREC_MIXED if p["precision"] == "mixed" else pkg.engine.PREC_FP64
+    opts = pkg.RunOpts(samples=samples or cfg["samples"], lanczos_steps=cfg["steps"],
+                       exact_block_threshold=cfg["threshold"], precision=prec,
+                       start_vector=pkg.engine.START_PHILOX_PHASE, batch_vectors=p["batch"])
+    mu = pkg.linspace(*cfg["mu"])
+    eng = pkg.Engine(model, opts)
+    try:
+        t0 = time.perf_counter()
+        eng.thermo_configure(cfg["betas"], mu)
+        n = model.sites
+        for nu in range(n + 1):
+            for nd in range(n + 1):
+                if sectors is not None and (nu, nd) not in sectors:
+                    continue
+                info = eng.sector_prepare(nu, nd)
+                blocks = [(k % model.lx, k // model.lx) for k, d in enumerate(info.block_dims) if d > 0]
+                exact = [b for b in blocks if info.block_dims[b[1] * model.lx + b[0]] <= cfg["threshold"]]
+                eng.blocks_exact_batched(exact)
+                eng.blocks_ftlm_batched([b for b in blocks if b not in exact])
+                for b in blocks:
+                    eng.thermo_accumulate_block(*b)
+        emin, z, ns, n2 = eng.thermo_read()
+        secs = time.perf_counter() - t0
+    finally:
+        eng.close()
+    b = np.asarray(cfg["betas"], np.float64).reshape(-1, 1)
+    return secs, {"n": ns / z / n, "log_partition": np.log(z) - b * emin}
+
+
+def run_curve_mode(args):
+    """--curve: seconds per n(mu) curve of the mixed batched path and of the
+    FP64 plain path, and |dn|, |d log Z| of mixed against FP64 with the same
+    Philox start vectors. With --plain-sectors the FP64 runs cover only those
+    sectors (the plain one with --plain-samples vectors; its time scales with
+    the vector count since each vector is its own sweep), the mixed curve is
+    still measured whole, and the FP64 curve times are extrapolated by the
+    FP64/mixed time ratios measured on exactly that work; |dn| is then the
+    difference of the grand-canonical sums over those sectors."""
+    import numpy as np
+    import ftlm_extended_hubbard_development_b200 as pkg
+    cfg = CURVES[args.curve]
+    S = cfg["samples"]
+    with ClockSampler(0) as clk:
+        t_mixed, c_mixed = time_curve(pkg, cfg, "mixed_batched")
+        if args.plain_sectors:
+            secs = [tuple(int(v) for v in x.split(",")) for x in args.plain_sectors.split(";")]
+            ns = args.plain_samples or S
+            tm, cm = time_curve(pkg, cfg, "mixed_batched", secs)
+            tb, cb = time_curve(pkg, cfg, "fp64_batched", secs)
+            tp, _ = time_curve(pkg, cfg, "fp64_plain", secs, ns)
+            tp_all = tp * S / ns
+            res = {"fp64_batched_s": t_mixed * tb / tm, "fp64_plain_s": t_mixed * tp_all / tm,
+                   "fp64_kind": "extrapolated",
+                   "fp64_basis": {"sectors": secs, "mixed_batched_s": tm, "fp64_batched_s": tb,
+                                  "fp64_plain_s": tp, "fp64_plain_samples": ns,
+                                  "fp64_plain_s_scaled_to_all_samples": tp_all},
+                   "dn_scope": "grand-canonical sums over the listed sectors"}
+        else:
+            tb, cb = time_curve(pkg, cfg, "fp64_batched")
+            tp, cp = time_curve(pkg, cfg, "fp64_plain")
+            cm = c_mixed
+            res = {"fp64_batched_s": tb, "fp64_plain_s": tp, "fp64_kind": "measured", "dn_scope": "whole curve",
+                   "dn_max_plain_vs_batched_fp64": float(np.abs(cp["n"] - cb["n"]).max())}
+    res["dn_max_mixed_vs_fp64"] = float(np.abs(cm["n"] - cb["n"]).max())
+    res["dlogz_max_mixed_vs_fp64"] = float(np.abs(cm["log_partition"] - cb["log_partition"]).max())
+    res["speedup_mixed_batched_vs_fp64_plain"] = res["fp64_plain_s"] / t_mixed
+    line = {"metric": "sec per n(mu) curve", "value": t_mixed, "unit": "s", "n_gpus": 1, "steps": 1, "warmup": 0,
+            "higher_is_better": False, "scaling": "none", "vs_baseline": None,
+            "dtype": "c64 vectors, f64 reductions", "data": "synthetic (model-defined; Philox start vectors)",
+            "config": {"workload": cfg["name"], **{k: v for k, v in cfg.items() if k != "name"}},
+            "curve": {"mixed_batched_s": t_mixed, **res}, "clocks": clk.summary()}
+    print(json.dumps(line))
+
+
 def main():
     global SECTOR, STEPS
     ap = argparse.ArgumentParser()
@@ -288,7 +389,13 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sector", default="8,8", help="N_up,N_down of the 4x4 sector (profiling cases)")
     ap.add_argument("--lanczos-steps", type=int, default=STEPS)
+    ap.add_argument("--curve", choices=sorted(CURVES), help="time whole n(mu) curves instead")
+    ap.add_argument("--plain-sectors", default="", help="'nu,nd;nu,nd': run the FP64 plain path on these only")
+    ap.add_argument("--plain-samples", type=int, default=0)
     args = ap.parse_args()
+    if args.curve:
+        run_curve_mode(args)
+        return
     SECTOR = tuple(int(x) for x in args.sector.split(","))
     STEPS = args.lanczos_steps
     if args.impl == "reference":

@@ -321,7 +321,6 @@ __global__ void __launch_bounds__(kHvThreads, MINB) k_hv(const __grid_constant__
   constexpr int CPR = NV / VPL;                 // 16-byte chunks per row
   constexpr int G = CPR < 32 ? CPR : 32;        // lanes per gathered row
   constexpr int LPL = CPR / G;                  // chunks per lane
-  constexpr int HPAR = 32 / G;                  // rows gathered in parallel
   constexpr bool kSmemBinom = sizeof(W) == 4;   // 64-bit words read C(n,k) from global/L1
   constexpr int kQ = queue_len<W>();
 
@@ -643,10 +642,9 @@ void launch_hv_t(Ctx& c, const void* in, void* out, const double* scale, double*
                                                                 scale, partial, gb);
 }
 
-// Kernel variants the autotuner chooses from: (gather unroll U, CTAs/SM).
+// Kernel variants the autotuner chooses from, (gather unroll U, CTAs/SM):
+// 0 (1,4), 1 (2,4), 2 (4,3), 3 (4,2), 4 (8,2).
 constexpr int kNumVariants = 5;
-constexpr int kVarU[kNumVariants] = {1, 2, 4, 4, 8};
-constexpr int kVarB[kNumVariants] = {4, 4, 3, 2, 2};
 
 template <typename W, typename R, typename T, int NV>
 void launch_hv_var(Ctx& c, int var, const void* in, void* out, const double* scale, double* partial, int grid) {
@@ -824,9 +822,6 @@ void block_csr(Ctx& c, std::vector<int32_t>& row_ptr, std::vector<int32_t>& col,
   dg.release();
 }
 
-// Grid of the H*V kernel: one warp per row when the block is small, else
-// a whole number of waves over the SMs (CTAs resident per SM from the
-// occupancy calculator), rows handed out round-robin to warps.
 // Grid of the H*V kernel: one warp per row for small blocks, else four CTAs
 // per SM (rows round-robin over warps). Independent of the kernel variant, so
 // the order of the per-CTA dot-product partials is too.
