@@ -260,6 +260,7 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "kernel": "k_hv (on-the-fly multi-vector H*V)",
+                         "kernel_variant": prof["hv_variant"],
                          "bytes_per_launch": bytes_per_launch,
                          "traffic": ncu_traffic()},
             "e2e": {"value": e2e_val, "unit": "GB/s",

@@ -199,9 +199,12 @@ int ftlm_sector_prepare(ftlm_ctx* ctx, int32_t n_up, int32_t n_down, ftlm_sector
     info.full_dim = static_cast<uint64_t>(c.sec.full_dim);
     info.parents = static_cast<uint64_t>(c.sec.parents);
     info.n_k = n;
+    c.block_dims.assign(n, 0);
     for (int my = 0; my < c.geom.ly; ++my)
-      for (int mx = 0; mx < c.geom.lx; ++mx)
-        info.block_dim[my * c.geom.lx + mx] = static_cast<uint64_t>(ftlm::block_dim_only(c, mx, my));
+      for (int mx = 0; mx < c.geom.lx; ++mx) {
+        c.block_dims[my * c.geom.lx + mx] = ftlm::block_dim_only(c, mx, my);
+        info.block_dim[my * c.geom.lx + mx] = static_cast<uint64_t>(c.block_dims[my * c.geom.lx + mx]);
+      }
     if (c.timing) {
       FTLM_CUDA(cudaEventRecord(e1, c.stream));
       FTLM_CUDA(cudaEventSynchronize(e1));
@@ -240,7 +243,7 @@ int ftlm_blocks_ftlm_batched(ftlm_ctx* ctx, const int32_t* mx, const int32_t* my
     std::vector<std::pair<int, int>> small, large;
     for (int i = 0; i < nblocks; ++i) {
       ftlm::check_k(c, mx[i], my[i]);
-      const int64_t d = ftlm::block_dim_only(c, mx[i], my[i]);
+      const int64_t d = c.block_dims[my[i] * c.geom.lx + mx[i]];
       if (d <= 0) continue;
       (c.small_blocks && d <= ftlm::kSmallMaxDim ? small : large).emplace_back(mx[i], my[i]);
     }

@@ -179,6 +179,7 @@ struct Ctx {
   DBuf binom;         // uint64 [65*65]
   DBuf binom32;       // uint32 [65*65]
   SectorTables sec;
+  std::vector<int64_t> block_dims;  // dimension of every k-block of the prepared sector (k = my*lx + mx)
   BlockTables blk;
   // Lanczos work space
   DBuf vec_a, vec_b, vec_h, partial, lz_alpha, lz_beta, lz_scale, lz_state, host_start;
@@ -231,6 +232,15 @@ void run_small_ftlm_blocks(Ctx& c, const std::vector<std::pair<int, int>>& block
 // nvmax vectors per sweep, steps[R] on the device) into the spectra arena.
 void ritz_stage(Ctx& c, int R, int nvmax, int ld, int K, const double* alpha, const double* beta,
                 const int32_t* steps, Spectrum& out);
+// The same for several blocks with one host synchronisation.
+struct RitzJob {
+  int R, nvmax, ld, K;
+  const double* alpha;
+  const double* beta;
+  const int32_t* steps;
+  Spectrum* out;
+};
+void ritz_stage_many(Ctx& c, std::vector<RitzJob>& jobs);
 // Exact spectra of several blocks of the prepared sector (one batched launch).
 void run_exact_blocks(Ctx& c, const std::vector<std::pair<int, int>>& blocks);
 // Thermo

@@ -423,40 +423,53 @@ void spectra_reset(Ctx& c) {
   c.spec.clear();
 }
 
-void ritz_stage(Ctx& c, int R, int nvmax, int ld, int K, const double* alpha, const double* beta,
-                const int32_t* steps, Spectrum& out) {
-  const int64_t off = spectra_alloc(c, 2 * static_cast<int64_t>(R) * K);
-  c.ritz_out.ensure(sizeof(double) * 3 * static_cast<size_t>(R) * K + 64);
-  double* dtmp = c.ritz_out.as<double>();
-  double* ztmp = dtmp + static_cast<size_t>(R) * K;
-  double* etmp = ztmp + static_cast<size_t>(R) * K;
-  int* status = reinterpret_cast<int*>(etmp + static_cast<size_t>(R) * K);
-  int64_t* total = reinterpret_cast<int64_t*>(status + 2);
-  FTLM_CUDA(cudaMemsetAsync(status, 0, sizeof(int), c.stream));
+void ritz_stage_many(Ctx& c, std::vector<RitzJob>& jobs) {
+  if (jobs.empty()) return;
+  // spectra slots first: spectra_alloc may move the arena
+  const size_t nj = jobs.size();
+  std::vector<int64_t> off(nj), scr(nj);
+  int64_t scr_tot = 0;
+  for (size_t i = 0; i < nj; ++i) {
+    off[i] = spectra_alloc(c, 2 * static_cast<int64_t>(jobs[i].R) * jobs[i].K);
+    scr[i] = scr_tot;
+    scr_tot += 3 * static_cast<int64_t>(jobs[i].R) * jobs[i].K;
+  }
+  c.ritz_out.ensure(sizeof(double) * scr_tot + sizeof(int64_t) * 2 * nj + 64);
+  double* scratch = c.ritz_out.as<double>();
+  int64_t* totals = reinterpret_cast<int64_t*>(scratch + scr_tot);  // [nj] counts, then [nj] status words
+  int* status = reinterpret_cast<int*>(totals + nj);
+  FTLM_CUDA(cudaMemsetAsync(status, 0, sizeof(int) * nj, c.stream));
   cudaEvent_t ee0 = nullptr, ee1 = nullptr;
   if (c.timing) {
     FTLM_CUDA(cudaEventCreate(&ee0));
     FTLM_CUDA(cudaEventCreate(&ee1));
     FTLM_CUDA(cudaEventRecord(ee0, c.stream));
   }
-  const size_t tsmem = sizeof(double) * 3 * 32 * static_cast<size_t>(K);
-  const int use_smem = tsmem <= 200 * 1024;
-  if (use_smem && tsmem > 48 * 1024)
-    FTLM_CUDA(cudaFuncSetAttribute(k_tridiag, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(tsmem)));
-  k_tridiag<<<(R + 31) / 32, 32, use_smem ? tsmem : 0, c.stream>>>(R, nvmax, ld, K, alpha, beta, steps, dtmp, ztmp,
-                                                                  etmp, 1.0 / R, status, use_smem);
+  for (size_t i = 0; i < nj; ++i) {
+    const RitzJob& jb = jobs[i];
+    const size_t rk = static_cast<size_t>(jb.R) * jb.K;
+    double* dtmp = scratch + scr[i];
+    double* ztmp = dtmp + rk;
+    double* etmp = ztmp + rk;
+    const size_t tsmem = sizeof(double) * 3 * 32 * static_cast<size_t>(jb.K);
+    const int use_smem = tsmem <= 200 * 1024;
+    if (use_smem && tsmem > 48 * 1024)
+      FTLM_CUDA(cudaFuncSetAttribute(k_tridiag, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(tsmem)));
+    k_tridiag<<<(jb.R + 31) / 32, 32, use_smem ? tsmem : 0, c.stream>>>(jb.R, jb.nvmax, jb.ld, jb.K, jb.alpha, jb.beta,
+                                                                       jb.steps, dtmp, ztmp, etmp, 1.0 / jb.R,
+                                                                       status + i, use_smem);
+    k_compact<<<1, 256, sizeof(int) * (jb.R + 1), c.stream>>>(
+        jb.R, jb.K, jb.steps, dtmp, ztmp, c.spectra.as<double>() + off[i],
+        c.spectra.as<double>() + off[i] + static_cast<int64_t>(rk), totals + i);
+    FTLM_LAUNCH_CHECK();
+    c.prof.kernel_launches += 2;
+  }
   if (c.timing) FTLM_CUDA(cudaEventRecord(ee1, c.stream));
-  k_compact<<<1, 256, sizeof(int) * (R + 1), c.stream>>>(R, K, steps, dtmp, ztmp, c.spectra.as<double>() + off,
-                                                          c.spectra.as<double>() + off + static_cast<int64_t>(R) * K,
-                                                          total);
-  FTLM_LAUNCH_CHECK();
-  c.prof.kernel_launches += 2;
-  int64_t cnt = 0;
-  int hstatus = 0;
-  FTLM_CUDA(cudaMemcpyAsync(&cnt, total, sizeof(int64_t), cudaMemcpyDeviceToHost, c.stream));
-  FTLM_CUDA(cudaMemcpyAsync(&hstatus, status, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  std::vector<int64_t> cnt(nj);
+  std::vector<int> hstatus(nj);
+  FTLM_CUDA(cudaMemcpyAsync(cnt.data(), totals, sizeof(int64_t) * nj, cudaMemcpyDeviceToHost, c.stream));
+  FTLM_CUDA(cudaMemcpyAsync(hstatus.data(), status, sizeof(int) * nj, cudaMemcpyDeviceToHost, c.stream));
   FTLM_CUDA(cudaStreamSynchronize(c.stream));
-  if (hstatus) throw Error(FTLM_ERR_NUMERIC, "tridiagonal QL did not converge");
   if (c.timing) {
     float ms = 0.f;
     FTLM_CUDA(cudaEventElapsedTime(&ms, ee0, ee1));
@@ -464,10 +477,20 @@ void ritz_stage(Ctx& c, int R, int nvmax, int ld, int K, const double* alpha, co
     cudaEventDestroy(ee0);
     cudaEventDestroy(ee1);
   }
-  out.ev_off = off;
-  out.w_off = off + static_cast<int64_t>(R) * K;
-  out.count = cnt;
-  out.exact = false;
+  for (size_t i = 0; i < nj; ++i) {
+    if (hstatus[i]) throw Error(FTLM_ERR_NUMERIC, "tridiagonal QL did not converge");
+    Spectrum& out = *jobs[i].out;
+    out.ev_off = off[i];
+    out.w_off = off[i] + static_cast<int64_t>(jobs[i].R) * jobs[i].K;
+    out.count = cnt[i];
+    out.exact = false;
+  }
+}
+
+void ritz_stage(Ctx& c, int R, int nvmax, int ld, int K, const double* alpha, const double* beta,
+                const int32_t* steps, Spectrum& out) {
+  std::vector<RitzJob> jobs{RitzJob{R, nvmax, ld, K, alpha, beta, steps, &out}};
+  ritz_stage_many(c, jobs);
 }
 
 void run_ftlm_block(Ctx& c, int n_up, int n_dn, int mx, int my, Spectrum& out, const double* host_start,

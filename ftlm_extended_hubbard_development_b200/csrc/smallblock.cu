@@ -197,8 +197,7 @@ void run_small_ftlm_blocks(Ctx& c, const std::vector<std::pair<int, int>>& block
   int ld = 1;  // alpha/beta row stride, as the sweep path uses for one sweep of R vectors
   while (ld < std::max(R, fp32 ? 2 : 1)) ld <<= 1;
   for (const auto& b : blocks) {
-    block_prepare(c, b.first, b.second);
-    const int64_t D = c.blk.dim;
+    const int64_t D = c.block_dims.at(static_cast<size_t>(b.second * c.geom.lx + b.first));
     if (D <= 0) continue;
     if (D > kSmallMaxDim) throw Error(FTLM_ERR_ARG, "block too large for the small-block FTLM launch");
     Item it{b.first, b.second, D, static_cast<int>(std::min<int64_t>(c.opts.lanczos_steps, D)), {}};
@@ -339,14 +338,20 @@ void run_small_ftlm_blocks(Ctx& c, const std::vector<std::pair<int, int>>& block
     cudaEventDestroy(e1);
   }
   // Ritz values and weights per block, then compaction into the spectra arena
-  for (Item& it : items) {
-    Spectrum s;
-    ritz_stage(c, R, R, ld, it.K, c.lz_alpha.as<double>() + it.d.ab_off, c.lz_beta.as<double>() + it.d.ab_off,
-               c.sb_steps.as<int32_t>() + it.d.steps_off, s);
-    s.prefactor = static_cast<double>(it.dim);
-    s.particles = c.sec.n_up + c.sec.n_dn;
-    s.dim = it.dim;
-    c.spec[{it.mx, it.my}] = s;
+  std::vector<Spectrum> spec(items.size());
+  std::vector<RitzJob> jobs;
+  for (size_t i = 0; i < items.size(); ++i) {
+    const Item& it = items[i];
+    jobs.push_back(RitzJob{R, R, ld, it.K, c.lz_alpha.as<double>() + it.d.ab_off,
+                           c.lz_beta.as<double>() + it.d.ab_off, c.sb_steps.as<int32_t>() + it.d.steps_off,
+                           &spec[i]});
+  }
+  ritz_stage_many(c, jobs);
+  for (size_t i = 0; i < items.size(); ++i) {
+    spec[i].prefactor = static_cast<double>(items[i].dim);
+    spec[i].particles = c.sec.n_up + c.sec.n_dn;
+    spec[i].dim = items[i].dim;
+    c.spec[{items[i].mx, items[i].my}] = spec[i];
   }
 }
 
