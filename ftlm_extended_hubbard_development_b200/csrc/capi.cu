@@ -165,7 +165,7 @@ void ftlm_ctx_destroy(ftlm_ctx* ctx) {
                         &c.sec.d_chi, &c.sec.d_cidx, &c.sec.canon, &c.sec.tmp_a, &c.sec.tmp_b, &c.sec.tmp_c,
                         &c.sec.tmp_d, &c.sec.tmp_e, &c.blk.act, &c.blk.act_list, &c.blk.aoff, &c.blk.dtab,
                         &c.blk.row_meta, &c.blk.row_dn, &c.vec_a, &c.vec_b, &c.vec_h, &c.partial,
-                        &c.lz_alpha, &c.lz_beta, &c.lz_scale, &c.lz_state, &c.host_start, &c.ritz_tmp, &c.ritz_out,
+                        &c.lz_alpha, &c.lz_beta, &c.lz_scale, &c.lz_state, &c.host_start, &c.ritz_tmp, &c.ritz_out, &c.ritz_meta,
                         &c.sb_rp, &c.sb_col, &c.sb_val, &c.sb_diag, &c.sb_meta, &c.sb_steps,
                         &c.scan_tmp, &c.dense_arena, &c.dense_meta, &c.dense_out, &c.spectra, &c.th_beta,
                         &c.th_mu, &c.th_state, &c.hl_ptr, &c.hl_ent};

@@ -183,7 +183,7 @@ struct Ctx {
   BlockTables blk;
   // Lanczos work space
   DBuf vec_a, vec_b, vec_h, partial, lz_alpha, lz_beta, lz_scale, lz_state, host_start;
-  DBuf ritz_tmp, ritz_out, scan_tmp;
+  DBuf ritz_tmp, ritz_out, ritz_meta, scan_tmp;
   // exact batch
   DBuf dense_arena, dense_meta, dense_out;
   // small-block FTLM batch: CSR arenas, task list, per-vector step counts

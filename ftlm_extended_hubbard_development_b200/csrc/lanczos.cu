@@ -213,21 +213,18 @@ struct Col {
   __device__ __forceinline__ double& operator[](int i) const { return p[i * st]; }
 };
 
-// Implicit QL with shifts on every Lanczos tridiagonal of a block (one
-// thread per random vector, all sweeps of the block in one launch), tracking
+// Implicit QL with shifts on every Lanczos tridiagonal (one thread per
+// random vector; k_tridiag_many serves all vectors of several blocks in one
+// launch, 32 vectors per CTA), tracking
 // the first row z of the eigenvector matrix; then an ascending sort.
 // alpha/beta are [sweep][K][ld] (vector r = sweep r/nvmax, lane r%nvmax),
 // steps[r] the alphas taken. Outputs eigenvalues and z^2 * inv_r into [R][K]
 // rows. With smem != 0 the three work columns of the warp's 32 vectors live
 // in shared memory ([3][K][32]), otherwise in global memory.
-__global__ void k_tridiag(int R, int nvmax, int ld, int K, const double* __restrict__ alpha,
-                          const double* __restrict__ beta, const int32_t* __restrict__ steps,
-                          double* __restrict__ dout, double* __restrict__ zout, double* __restrict__ escr,
-                          double inv_r, int* __restrict__ status, int smem) {
-  extern __shared__ double sm[];
-  const int t = threadIdx.x;
-  const int r = blockIdx.x * blockDim.x + t;
-  if (r >= R) return;
+__device__ void tridiag_vector(int r, int t, int nvmax, int ld, int K, const double* __restrict__ alpha,
+                               const double* __restrict__ beta, const int32_t* __restrict__ steps,
+                               double* __restrict__ dout, double* __restrict__ zout, double* __restrict__ escr,
+                               double inv_r, int* __restrict__ status, double* sm, int smem) {
   const int n = steps[r];
   const int64_t base = (static_cast<int64_t>(r / nvmax) * K) * ld + r % nvmax;
   Col d, z, e;
@@ -312,12 +309,34 @@ __global__ void k_tridiag(int R, int nvmax, int ld, int K, const double* __restr
   }
 }
 
+// Several blocks' Ritz stages in one launch: CTA b belongs to the job j with
+// cta0[j] <= b < cta0[j+1] and serves that job's vectors 32(b-cta0[j]) ...
+struct RitzJobDev {
+  int R, nvmax, ld, K, cta0, pad;
+  const double* alpha;
+  const double* beta;
+  const int32_t* steps;
+  double *dout, *zout, *escr, *ev_out, *w_out;
+  int64_t* total;
+  int* status;
+};
+
+__global__ void k_tridiag_many(int njobs, const RitzJobDev* __restrict__ jobs, int smem) {
+  extern __shared__ double sm[];
+  int j = 0;
+  while (j + 1 < njobs && jobs[j + 1].cta0 <= static_cast<int>(blockIdx.x)) ++j;
+  const RitzJobDev J = jobs[j];
+  const int r = (blockIdx.x - J.cta0) * blockDim.x + threadIdx.x;
+  if (r >= J.R) return;
+  tridiag_vector(r, threadIdx.x, J.nvmax, J.ld, J.K, J.alpha, J.beta, J.steps, J.dout, J.zout, J.escr, 1.0 / J.R,
+                 J.status, sm, smem);
+}
+
 // Concatenate the per-vector spectra sample by sample (main.cpp:1097-1110).
 // Dynamic shared memory: R+1 offsets.
-__global__ void k_compact(int R, int K, const int32_t* __restrict__ steps, const double* __restrict__ d,
-                          const double* __restrict__ w, double* __restrict__ ev_out, double* __restrict__ w_out,
-                          int64_t* __restrict__ total) {
-  extern __shared__ int off[];
+__device__ void compact_block(int R, int K, const int32_t* __restrict__ steps, const double* __restrict__ d,
+                              const double* __restrict__ w, double* __restrict__ ev_out, double* __restrict__ w_out,
+                              int64_t* __restrict__ total, int* off) {
   if (threadIdx.x == 0) {
     int o = 0;
     for (int v = 0; v < R; ++v) {
@@ -335,6 +354,13 @@ __global__ void k_compact(int R, int K, const int32_t* __restrict__ steps, const
       w_out[off[v] + i] = w[static_cast<int64_t>(v) * K + i];
     }
   }
+}
+
+// One CTA per job.
+__global__ void k_compact_many(const RitzJobDev* __restrict__ jobs) {
+  extern __shared__ int off[];
+  const RitzJobDev J = jobs[blockIdx.x];
+  compact_block(J.R, J.K, J.steps, J.dout, J.zout, J.ev_out, J.w_out, J.total, off);
 }
 
 // Steps of the nva vectors of one sweep, into the block's [R] array.
@@ -445,25 +471,44 @@ void ritz_stage_many(Ctx& c, std::vector<RitzJob>& jobs) {
     FTLM_CUDA(cudaEventCreate(&ee1));
     FTLM_CUDA(cudaEventRecord(ee0, c.stream));
   }
+  std::vector<RitzJobDev> dj(nj);
+  int ctas = 0, kmax = 1, rmax = 1;
   for (size_t i = 0; i < nj; ++i) {
     const RitzJob& jb = jobs[i];
     const size_t rk = static_cast<size_t>(jb.R) * jb.K;
-    double* dtmp = scratch + scr[i];
-    double* ztmp = dtmp + rk;
-    double* etmp = ztmp + rk;
-    const size_t tsmem = sizeof(double) * 3 * 32 * static_cast<size_t>(jb.K);
-    const int use_smem = tsmem <= 200 * 1024;
-    if (use_smem && tsmem > 48 * 1024)
-      FTLM_CUDA(cudaFuncSetAttribute(k_tridiag, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(tsmem)));
-    k_tridiag<<<(jb.R + 31) / 32, 32, use_smem ? tsmem : 0, c.stream>>>(jb.R, jb.nvmax, jb.ld, jb.K, jb.alpha, jb.beta,
-                                                                       jb.steps, dtmp, ztmp, etmp, 1.0 / jb.R,
-                                                                       status + i, use_smem);
-    k_compact<<<1, 256, sizeof(int) * (jb.R + 1), c.stream>>>(
-        jb.R, jb.K, jb.steps, dtmp, ztmp, c.spectra.as<double>() + off[i],
-        c.spectra.as<double>() + off[i] + static_cast<int64_t>(rk), totals + i);
-    FTLM_LAUNCH_CHECK();
-    c.prof.kernel_launches += 2;
+    RitzJobDev& d = dj[i];
+    d.R = jb.R;
+    d.nvmax = jb.nvmax;
+    d.ld = jb.ld;
+    d.K = jb.K;
+    d.cta0 = ctas;
+    d.pad = 0;
+    d.alpha = jb.alpha;
+    d.beta = jb.beta;
+    d.steps = jb.steps;
+    d.dout = scratch + scr[i];
+    d.zout = d.dout + rk;
+    d.escr = d.zout + rk;
+    d.ev_out = c.spectra.as<double>() + off[i];
+    d.w_out = d.ev_out + rk;
+    d.total = totals + i;
+    d.status = status + i;
+    ctas += (jb.R + 31) / 32;
+    kmax = std::max(kmax, jb.K);
+    rmax = std::max(rmax, jb.R);
   }
+  c.ritz_meta.ensure(sizeof(RitzJobDev) * nj);
+  FTLM_CUDA(cudaMemcpyAsync(c.ritz_meta.p, dj.data(), sizeof(RitzJobDev) * nj, cudaMemcpyHostToDevice, c.stream));
+  const size_t tsmem = sizeof(double) * 3 * 32 * static_cast<size_t>(kmax);
+  const int use_smem = tsmem <= 200 * 1024;
+  if (use_smem && tsmem > 48 * 1024)
+    FTLM_CUDA(cudaFuncSetAttribute(k_tridiag_many, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(tsmem)));
+  k_tridiag_many<<<ctas, 32, use_smem ? tsmem : 0, c.stream>>>(static_cast<int>(nj), c.ritz_meta.as<RitzJobDev>(),
+                                                              use_smem);
+  k_compact_many<<<static_cast<int>(nj), 256, sizeof(int) * (rmax + 1), c.stream>>>(c.ritz_meta.as<RitzJobDev>());
+  FTLM_LAUNCH_CHECK();
+  c.prof.kernel_launches += 2;
   if (c.timing) FTLM_CUDA(cudaEventRecord(ee1, c.stream));
   std::vector<int64_t> cnt(nj);
   std::vector<int> hstatus(nj);
