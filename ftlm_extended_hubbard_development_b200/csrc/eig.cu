@@ -1,7 +1,9 @@
 // Exact block spectra on the GPU (diagonalize_block_exact, main.cpp:847-911).
 //
 // Every block of the list is assembled as a dense column-major Hermitian
-// matrix from its device CSR, symmetrised as (M + M^H)/2 like the
+// matrix straight from its hop enumeration (the CSR's entries, summed in
+// the CSR's order, with no CSR stored and no host synchronisation between
+// blocks), symmetrised as (M + M^H)/2 like the
 // reference, then all matrices are diagonalised by ONE batched launch:
 // one CTA per matrix (largest first) reduces it to real symmetric
 // tridiagonal form with complex Householder reflections (trailing
@@ -21,21 +23,6 @@ namespace {
 
 constexpr int kEigThreads = 256;
 constexpr int kMaxDense = 7000;  // two complex work vectors in shared memory: 2*7000*16 B <= 227 KB
-
-__global__ void k_dense_build(int64_t n, const int32_t* __restrict__ rp, const int32_t* __restrict__ col,
-                              const double2* __restrict__ val, const double* __restrict__ diag,
-                              double2* __restrict__ A) {
-  // row i of M -> A[i + j*n]; one thread per row keeps the entry order
-  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
-       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    A[i + i * n].x += diag[i];
-    for (int32_t e = rp[i]; e < rp[i + 1]; ++e) {
-      double2& a = A[i + static_cast<int64_t>(col[e]) * n];
-      a.x += val[e].x;
-      a.y += val[e].y;
-    }
-  }
-}
 
 // (M + M^H)/2 with a real diagonal (main.cpp:875-886); upper triangle
 // holds the average, the lower triangle its conjugate.
@@ -245,25 +232,18 @@ void run_exact_blocks(Ctx& c, const std::vector<std::pair<int, int>>& blocks) {
     FTLM_CUDA(cudaEventCreate(&e1));
     FTLM_CUDA(cudaEventRecord(e0, c.stream));
   }
-  DBuf rp, cl, vl, dg;
+  for (Item& it : items) it.eoff = spectra_alloc(c, it.n);
   for (Item& it : items) {
+    // the block's rows are built in stream order; the fill reads them before
+    // the next block_prepare overwrites them
     block_prepare(c, it.mx, it.my);
-    block_csr_device(c, rp, cl, vl, dg);
     double2* A = c.dense_arena.as<double2>() + it.aoff;
-    const int g1 = static_cast<int>(std::min<int64_t>((it.n + 127) / 128, 4096));
-    k_dense_build<<<g1, 128, 0, c.stream>>>(it.n, rp.as<int32_t>(), cl.as<int32_t>(), vl.as<double2>(), dg.as<double>(), A);
+    block_dense_device(c, A);
     const int g2 = static_cast<int>(std::min<int64_t>((it.n * it.n + 255) / 256, 4096));
     k_dense_herm<<<g2, 256, 0, c.stream>>>(it.n, A);
     FTLM_LAUNCH_CHECK();
-    c.prof.kernel_launches += 2;
-    it.eoff = spectra_alloc(c, it.n);
-    // dense_build reads rp/cl/vl before they are rebuilt for the next block
-    FTLM_CUDA(cudaStreamSynchronize(c.stream));
+    c.prof.kernel_launches += 1;
   }
-  rp.release();
-  cl.release();
-  vl.release();
-  dg.release();
   if (c.timing) {
     FTLM_CUDA(cudaEventRecord(e1, c.stream));
     FTLM_CUDA(cudaEventSynchronize(e1));

@@ -213,6 +213,9 @@ void block_csr(Ctx& c, std::vector<int32_t>& row_ptr, std::vector<int32_t>& col,
                std::vector<double>& val, std::vector<double>& diag);
 // Device CSR of the prepared block (reference entry order); returns nnz.
 int64_t block_csr_device(Ctx& c, DBuf& row_ptr, DBuf& col, DBuf& val, DBuf& diag);
+// Dense column-major matrix of the prepared block added into A (zeroed by the
+// caller), entries summed in the CSR's order; no host synchronisation.
+void block_dense_device(Ctx& c, double2* A);
 // H*V of the prepared block on device arrays [dim][nv] complex (FP64 or FP32).
 void hv_apply(Ctx& c, const void* in, void* out, int nv, bool fp32, const double* scale_dev,
               double* partial_dev, int nblocks_hint);

@@ -79,6 +79,10 @@ struct CsrParams {
 
 // One thread per row, hops in reference order: up spin first, occupied
 // source sites ascending, directions 0..7, zero-amplitude hops included.
+// fill 0: count entries; 1: write the CSR; 2: count nonzero-amplitude hops;
+// 3: add the row straight into a dense column-major matrix (val as double2
+// A[row + col*dim], zeroed by the caller): diagonal first, then the entries
+// in CSR order, which is the sum order of building it from the CSR.
 template <typename W>
 __global__ void k_csr(const __grid_constant__ CsrParams<W> P, const uint64_t* __restrict__ binom, int fill,
                       int32_t* __restrict__ counts, const int64_t* __restrict__ row_ptr, int32_t* __restrict__ col,
@@ -93,6 +97,10 @@ __global__ void k_csr(const __grid_constant__ CsrParams<W> P, const uint64_t* __
     const W u = v.ur_bits[ur];
     const W d = v.row_dn[i];
     int64_t pos = fill == 1 ? row_ptr[i] : 0;  // row_ptr exists only in the fill pass
+    if (fill == 3) {
+      double2* a = reinterpret_cast<double2*>(val) + (i + i * v.dim);
+      a->x = __dadd_rn(a->x, diag_energy(u, d, g));
+    }
     int cnt = 0;
     for (int spin = 0; spin < 2; ++spin) {
       const W bits = spin ? d : u;
@@ -108,7 +116,7 @@ __global__ void k_csr(const __grid_constant__ CsrParams<W> P, const uint64_t* __
           if (!resolve<W, uint64_t>(spin ? u : moved, spin ? moved : d, spin == 0, ur, v, g, binom, c, shift,
                                     sgn, deg_t))
             continue;
-          if (fill == 1) {
+          if (fill == 1 || fill == 3) {
             const int p = jw_parity(bits, from, to) ^ sgn;
             // ((amp * sign) * phase) * ratio, the operation order of main.cpp:794-797
             const double ar = p ? -g.amp_re[dir] : g.amp_re[dir];
@@ -117,17 +125,23 @@ __global__ void k_csr(const __grid_constant__ CsrParams<W> P, const uint64_t* __
             const double re = __dsub_rn(__dmul_rn(ar, pr), __dmul_rn(ai, pi));
             const double im = __dadd_rn(__dmul_rn(ar, pi), __dmul_rn(ai, pr));
             const double ratio = __ddiv_rn(g.sqrt_deg[deg_t], g.sqrt_deg[deg_s]);
-            col[pos] = static_cast<int32_t>(c);
-            val[2 * pos] = __dmul_rn(re, ratio);
-            val[2 * pos + 1] = __dmul_rn(im, ratio);
-            ++pos;
+            if (fill == 1) {
+              col[pos] = static_cast<int32_t>(c);
+              val[2 * pos] = __dmul_rn(re, ratio);
+              val[2 * pos + 1] = __dmul_rn(im, ratio);
+              ++pos;
+            } else {
+              double2* a = reinterpret_cast<double2*>(val) + (i + c * v.dim);
+              a->x = __dadd_rn(a->x, __dmul_rn(re, ratio));
+              a->y = __dadd_rn(a->y, __dmul_rn(im, ratio));
+            }
           }
           ++cnt;
         }
       }
     }
     if (fill == 1) diag[i] = diag_energy(u, d, g);
-    else counts[i] = cnt;
+    else if (fill != 3) counts[i] = cnt;
   }
 }
 
@@ -737,6 +751,18 @@ int64_t block_csr_device_t(Ctx& c, DBuf& row_ptr, DBuf& col, DBuf& val, DBuf& di
 }
 
 template <typename W>
+void block_dense_device_t(Ctx& c, double2* A) {
+  CsrParams<W> P;
+  P.g = c.geom;
+  if constexpr (sizeof(W) == 4) P.v = view32(c);
+  else P.v = view64(c);
+  k_csr<W><<<grid_for(c.blk.dim, 128), 128, 0, c.stream>>>(P, c.binom.as<uint64_t>(), 3, nullptr, nullptr, nullptr,
+                                                            reinterpret_cast<double*>(A), nullptr);
+  FTLM_LAUNCH_CHECK();
+  c.prof.kernel_launches += 1;
+}
+
+template <typename W>
 int64_t block_nonzero_hops_t(Ctx& c) {
   const int64_t D = c.blk.dim;
   if (D <= 0) return 0;
@@ -799,6 +825,11 @@ int64_t block_nonzero_hops(Ctx& c) {
 int64_t block_csr_device(Ctx& c, DBuf& row_ptr, DBuf& col, DBuf& val, DBuf& diag) {
   if (c.wide) return block_csr_device_t<uint64_t>(c, row_ptr, col, val, diag);
   return block_csr_device_t<uint32_t>(c, row_ptr, col, val, diag);
+}
+
+void block_dense_device(Ctx& c, double2* A) {
+  if (c.wide) block_dense_device_t<uint64_t>(c, A);
+  else block_dense_device_t<uint32_t>(c, A);
 }
 
 void block_csr(Ctx& c, std::vector<int32_t>& row_ptr, std::vector<int32_t>& col, std::vector<double>& val,
