@@ -580,13 +580,15 @@ int run_ftlm_main(int argc, char** argv) {  // main.cpp:1459-1839
           }
         eng.check(ftlm_blocks_exact_batched(eng.ctx(), ex_mx.data(), ex_my.data(), static_cast<int>(ex_mx.size())),
                   "blocks_exact_batched");
-        // and every FTLM spectrum of blocks without exact/trace/debug output
+        // and every FTLM spectrum of blocks without exact/trace/debug output;
+        // with a checkpoint only the small ones, so that a large block is
+        // still written to the checkpoint as soon as it is done
         std::vector<int32_t> ft_mx, ft_my;
         for (int my = 0; my < params.ly; ++my)
           for (int mx = 0; mx < params.lx; ++mx) {
             const uint64_t dim = info.block_dim[my * params.lx + mx];
             if (dim == 0 || dim <= params.exact_block_threshold || ckpt.count(BlockKey{n_up, n_down, mx, my}) ||
-                trace_blocks || matches(mx, my))
+                trace_blocks || matches(mx, my) || (!params.checkpoint.empty() && dim > FTLM_SMALL_BLOCK_MAX))
               continue;
             ft_mx.push_back(mx);
             ft_my.push_back(my);
