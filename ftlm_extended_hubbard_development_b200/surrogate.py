@@ -41,6 +41,7 @@ whose mean is the prediction.
 from __future__ import annotations
 
 import math
+import time
 from dataclasses import dataclass, replace
 
 import numpy as np
@@ -308,13 +309,21 @@ def surrogate_twist_average(model: Model, betas, mu, opts: RunOpts, grid=6, held
     every judge passes (max |dn| <= threshold); otherwise average the
     engine's own curves at the training and held-out twists (fallback)."""
     opts = replace(opts, device=device)
+    t0 = time.perf_counter()
     train = [collect(model, px, py, betas, mu, opts, ed, levels) for px, py in uniform_grid(grid)]
+    t1 = time.perf_counter()
     sur = TwistSurrogate(model, levels=levels, members=members, device=device)
     hist = sur.fit(train, betas, mu, epochs=epochs)
+    t2 = time.perf_counter()
     judges = []
+    t_judge = t_pred = 0.0
     for px, py in heldout_twists(heldout, seed):
+        ta = time.perf_counter()
         td = collect(model, px, py, betas, mu, opts, ed, levels)
+        tb = time.perf_counter()
         pred = sur.curve(px, py, betas, mu)
+        t_judge += tb - ta
+        t_pred += time.perf_counter() - tb
         near = sur.nearest(px, py, wrap=True)  # the curve without the network
         judges.append({"twist": (px, py), "curve": td.curve,
                        "err_surrogate": float(np.abs(pred["n"] - td.curve["n"]).max()),
@@ -334,6 +343,77 @@ def surrogate_twist_average(model: Model, betas, mu, opts: RunOpts, grid=6, held
     grid_rows = []
     for td in train:
         grid_rows += curve_rows(td.curve, betas, mu)
+    timing = {"engine_s_per_twist": (t1 - t0 + t_judge) / max(len(train) + len(judges), 1),
+              "training_s": t2 - t1, "surrogate_s_per_twist": t_pred / max(len(judges), 1)}
     return {"average": combine_rows(rows, "observable-average"), "source": source, "accepted": accepted,
             "judges": judges, "loss_history": hist, "training_grid_average": combine_rows(grid_rows),
-            "surrogate": sur, "train": train}
+            "surrogate": sur, "train": train, "timing": timing}
+
+
+def main(argv=None):
+    """Command line: the surrogate twist average of one model, with a JSON
+    summary (judges' errors, the nearest-twist baseline, timings) on stdout
+    and the averaged curve as CSV (twist.py's columns)."""
+    import argparse
+    import json
+
+    from .engine import PREC_FP64, PREC_MIXED, START_PHILOX_PHASE, START_REF_GAUSSIAN, linspace
+    from .twist import write_rows
+
+    ap = argparse.ArgumentParser(description="Twist average of n(mu) with the learned surrogate")
+    ap.add_argument("--lx", type=int, default=4)
+    ap.add_argument("--ly", type=int, default=4)
+    ap.add_argument("--tx", type=float, default=1.0)
+    ap.add_argument("--ty", type=float, default=1.0)
+    ap.add_argument("--tp", type=float, default=-0.25)
+    ap.add_argument("--u", type=float, default=7.0)
+    ap.add_argument("--v", type=float, default=1.0)
+    ap.add_argument("--beta-list", default="5")
+    ap.add_argument("--mu-min", type=float, default=-3.0)
+    ap.add_argument("--mu-max", type=float, default=4.0)
+    ap.add_argument("--mu-points", type=int, default=141)
+    ap.add_argument("--samples", type=int, default=128)
+    ap.add_argument("--lanczos-steps", type=int, default=80)
+    ap.add_argument("--exact-block-threshold", type=int, default=256)
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
+    ap.add_argument("--start-vector", choices=["ref-gaussian", "philox-phase"], default="philox-phase")
+    ap.add_argument("--ed", action="store_true", help="diagonalise every block exactly")
+    ap.add_argument("--grid", type=int, default=6)
+    ap.add_argument("--heldout", type=int, default=8)
+    ap.add_argument("--dense", type=int, default=24)
+    ap.add_argument("--threshold", type=float, default=0.01)
+    ap.add_argument("--epochs", type=int, default=600)
+    ap.add_argument("--members", type=int, default=MEMBERS)
+    ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--output", help="CSV of the twist-averaged curve")
+    a = ap.parse_args(argv)
+    model = Model(lx=a.lx, ly=a.ly, tx=a.tx, ty=a.ty, tp=a.tp, u=a.u, v=a.v)
+    betas = [float(b) for b in a.beta_list.split(",")]
+    mu = linspace(a.mu_min, a.mu_max, a.mu_points)
+    opts = RunOpts(samples=a.samples, lanczos_steps=a.lanczos_steps, exact_block_threshold=a.exact_block_threshold,
+                   precision=PREC_MIXED if a.precision == "mixed" else PREC_FP64,
+                   start_vector=START_PHILOX_PHASE if a.start_vector == "philox-phase" else START_REF_GAUSSIAN)
+    res = surrogate_twist_average(model, betas, mu, opts, grid=a.grid, heldout=a.heldout, dense=a.dense,
+                                  threshold=a.threshold, ed=a.ed, epochs=a.epochs, members=a.members,
+                                  device=a.device)
+    es = np.array([j["err_surrogate"] for j in res["judges"]])
+    en = np.array([j["err_nearest_twist"] for j in res["judges"]])
+    g = np.array([r["n"] for r in res["training_grid_average"]])
+    avg = np.array([r["n"] for r in res["average"]])
+    print(json.dumps({"model": model.__dict__, "betas": betas, "mu": [a.mu_min, a.mu_max, a.mu_points],
+                      "samples": a.samples, "lanczos_steps": a.lanczos_steps, "ed": a.ed, "grid": a.grid,
+                      "heldout": a.heldout, "threshold": a.threshold, "accepted": res["accepted"],
+                      "source": res["source"], "judge_max_dn_surrogate": es.round(6).tolist(),
+                      "judge_max_dn_nearest_twist": en.round(6).tolist(),
+                      "loss_first_last": [float(res["loss_history"][0]), float(res["loss_history"][-1])],
+                      "max_dn_average_vs_training_grid_average": float(np.abs(avg - g).max()),
+                      **res["timing"]}))
+    if a.output:
+        write_rows(a.output, res["average"])
+    res["surrogate"].close()
+    return 0
+
+
+if __name__ == "__main__":
+    import sys
+    sys.exit(main())
