@@ -303,15 +303,22 @@ def heldout_twists(count=8, seed=2024):
 
 def surrogate_twist_average(model: Model, betas, mu, opts: RunOpts, grid=6, heldout=8, dense=24,
                             threshold=0.01, ed=False, epochs=600, seed=2024, levels=LEVELS, members=MEMBERS,
-                            device=0):
+                            device=0, log=None):
     """Train on a grid x grid twist set, judge at `heldout` Philox twists with
     the engine, and average n(mu) over the surrogate's dense x dense grid when
     every judge passes (max |dn| <= threshold); otherwise average the
     engine's own curves at the training and held-out twists (fallback)."""
     opts = replace(opts, device=device)
     t0 = time.perf_counter()
-    train = [collect(model, px, py, betas, mu, opts, ed, levels) for px, py in uniform_grid(grid)]
+    train = []
+    for px, py in uniform_grid(grid):
+        train.append(collect(model, px, py, betas, mu, opts, ed, levels))
+        if log:
+            log(f"training twist {len(train)}/{grid * grid} ({px:.4f}, {py:.4f}) "
+                f"at {time.perf_counter() - t0:.1f} s")
     t1 = time.perf_counter()
+    if log:
+        log(f"training the surrogate on {len(train)} twists")
     sur = TwistSurrogate(model, levels=levels, members=members, device=device)
     hist = sur.fit(train, betas, mu, epochs=epochs)
     t2 = time.perf_counter()
@@ -324,6 +331,8 @@ def surrogate_twist_average(model: Model, betas, mu, opts: RunOpts, grid=6, held
         pred = sur.curve(px, py, betas, mu)
         t_judge += tb - ta
         t_pred += time.perf_counter() - tb
+        if log:
+            log(f"judge twist ({px:.4f}, {py:.4f}): engine {tb - ta:.1f} s")
         near = sur.nearest(px, py, wrap=True)  # the curve without the network
         judges.append({"twist": (px, py), "curve": td.curve,
                        "err_surrogate": float(np.abs(pred["n"] - td.curve["n"]).max()),
@@ -356,6 +365,7 @@ def main(argv=None):
     and the averaged curve as CSV (twist.py's columns)."""
     import argparse
     import json
+    import sys
 
     from .engine import PREC_FP64, PREC_MIXED, START_PHILOX_PHASE, START_REF_GAUSSIAN, linspace
     from .twist import write_rows
@@ -395,7 +405,7 @@ def main(argv=None):
                    start_vector=START_PHILOX_PHASE if a.start_vector == "philox-phase" else START_REF_GAUSSIAN)
     res = surrogate_twist_average(model, betas, mu, opts, grid=a.grid, heldout=a.heldout, dense=a.dense,
                                   threshold=a.threshold, ed=a.ed, epochs=a.epochs, members=a.members,
-                                  device=a.device)
+                                  device=a.device, log=lambda m: print(m, file=sys.stderr, flush=True))
     es = np.array([j["err_surrogate"] for j in res["judges"]])
     en = np.array([j["err_nearest_twist"] for j in res["judges"]])
     g = np.array([r["n"] for r in res["training_grid_average"]])
