@@ -333,6 +333,41 @@ def time_curve(pkg, cfg, path, sectors=None, samples=None):
     return secs, {"n": ns / z / n, "log_partition": np.log(z) - b * emin}
 
 
+def run_curve_reference(args):
+    """--curve config2 --impl reference: the reference's own executable
+    (compiled from its sources into oracle/_ref) on the config-2 curve with
+    all host threads, wall time per curve. Config 3 is out of its reach
+    (the (8,8) sector alone needs ~15 min and ~30 GB to build on the CPU)."""
+    cfg = CURVES[args.curve]
+    exe = os.path.join(HERE, "oracle", "_ref", "ftlm_n_vs_mu")
+    if args.curve != "config2" or not os.path.exists(exe):
+        why = "config3 exceeds the reference's CPU memory/time" if args.curve != "config2" else \
+              "oracle/_ref/ftlm_n_vs_mu not built (make -C oracle ref)"
+        print(json.dumps({"impl": "reference", "unavailable": why}))
+        return
+    m = cfg["model"]
+    threads = os.cpu_count() or 1
+    cmd = [exe, "--lx", str(m["lx"]), "--ly", str(m["ly"]), "--tx", repr(m["tx"]), "--ty", repr(m["ty"]),
+           "--tp", repr(m["tp"]), "--u", repr(m["u"]), "--v", repr(m["v"]), "--beta", repr(cfg["betas"][0]),
+           "--mu-min", repr(cfg["mu"][0]), "--mu-max", repr(cfg["mu"][1]), "--mu-count", str(cfg["mu"][2]),
+           "--samples", str(cfg["samples"]), "--lanczos-steps", str(cfg["steps"]),
+           "--exact-block-threshold", str(cfg["threshold"]), "--threads", str(threads)]
+    import tempfile
+    with tempfile.TemporaryDirectory() as d:
+        t0 = time.perf_counter()
+        r = subprocess.run(cmd + ["--output", os.path.join(d, "n.csv")], capture_output=True, text=True)
+        secs = time.perf_counter() - t0
+    if r.returncode != 0:
+        print(json.dumps({"impl": "reference", "unavailable": "reference run failed: " + r.stderr[-200:]}))
+        return
+    print(json.dumps({"metric": "sec per n(mu) curve", "value": secs, "unit": "s", "n_gpus": 0, "steps": 1,
+                      "warmup": 0, "higher_is_better": False, "impl": "reference",
+                      "config": {"workload": cfg["name"]},
+                      "cpu_baseline": {"value": secs, "unit": "s", "cores": threads, "kind": "reference",
+                                       "sample": "whole config-2 curve, reference ftlm_n_vs_mu (OpenMP)"},
+                      "e2e": {"value": secs, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
 def run_curve_mode(args):
     """--curve: seconds per n(mu) curve of the mixed batched path and of the
     FP64 plain path, and |dn|, |d log Z| of mixed against FP64 with the same
@@ -395,7 +430,10 @@ def main():
     ap.add_argument("--plain-samples", type=int, default=0)
     args = ap.parse_args()
     if args.curve:
-        run_curve_mode(args)
+        if args.impl == "reference":
+            run_curve_reference(args)
+        else:
+            run_curve_mode(args)
         return
     SECTOR = tuple(int(x) for x in args.sector.split(","))
     STEPS = args.lanczos_steps
