@@ -108,10 +108,11 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def ncu_traffic():
+def ncu_traffic(args):
     """DRAM bytes per H*V launch of the bench block, from the committed
-    one-pass ncu summary (profiles/k_hv_4x4_sector88_nv128_mixed_traffic.md)."""
-    if SECTOR != (8, 8) or STEPS <= 0:
+    one-pass ncu summary (profiles/k_hv_4x4_sector88_nv128_mixed_traffic.md);
+    None for any other workload than the default one it was captured on."""
+    if SECTOR != (8, 8) or STEPS <= 0 or args.precision != "mixed" or args.batch not in (0, 128):
         return None
     p = os.path.join(HERE, "profiles", "k_hv_4x4_sector88_nv128_mixed_traffic.md")
     try:
@@ -259,10 +260,11 @@ def run_ours(args):
                        "parallelism": f"weak: one k-block per rank x{ws}"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
-                         "kernel": "k_hv (on-the-fly multi-vector H*V)",
+                         "kernel": ("k_hv_list (cached hop list)" if 0 < args.batch <= 32
+                                    else "k_hv (on-the-fly multi-vector H*V)"),
                          "kernel_variant": prof["hv_variant"],
                          "bytes_per_launch": bytes_per_launch,
-                         "traffic": ncu_traffic()},
+                         "traffic": ncu_traffic(args)},
             "e2e": {"value": e2e_val, "unit": "GB/s",
                     "h2d_bytes_per_step": pe["h2d_bytes"] / args.steps,
                     "d2h_bytes_per_step": pe["d2h_bytes"] / args.steps},
