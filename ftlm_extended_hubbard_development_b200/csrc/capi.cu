@@ -135,6 +135,7 @@ int ftlm_ctx_create(const ftlm_model* model, const ftlm_run_opts* opts, ftlm_ctx
   if (const char* hm = std::getenv("FTLM_HV_MODE"))
     c.hv_mode = std::string(hm) == "list" ? 1 : (std::string(hm) == "fly" ? 0 : -1);
   if (const char* sb = std::getenv("FTLM_SMALL_BLOCKS")) c.small_blocks = std::string(sb) != "0";
+  if (const char* hr = std::getenv("FTLM_HV_ROWS")) c.hv_rows = std::string(hr) != "0";
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0 || c.device < 0 || c.device >= ndev) {
     cudaGetLastError();

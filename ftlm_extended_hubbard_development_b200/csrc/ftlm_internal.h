@@ -169,6 +169,7 @@ struct Ctx {
   int hv_forced = -1; // H*V kernel variant forced by FTLM_HV_VARIANT (-1: autotune)
   int hv_mode = -1;   // H*V operator source: -1 auto, 0 on-the-fly lookups, 1 cached hop list (FTLM_HV_MODE)
   bool hl_active = false;  // H*V kernels read the cached hop list of the prepared block
+  bool hv_rows = true;  // narrow sweeps on the hop list: 8 lanes per row (FTLM_HV_ROWS=0: warp per row)
   bool small_blocks = true;  // batched FTLM runs blocks <= kSmallMaxDim in one launch (FTLM_SMALL_BLOCKS=0: off)
   int64_t hl_nnz = 0;
   DBuf hl_ptr, hl_ent;     // hop list: int64 row pointers, packed uint64 entries

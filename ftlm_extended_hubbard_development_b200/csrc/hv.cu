@@ -638,6 +638,131 @@ __global__ void __launch_bounds__(kHvThreads, MINB) k_hv_list(const __grid_const
   }
 }
 
+// H*V from the cached hop list for sweeps whose row is one 16-byte chunk
+// (2 FP32 or 1 FP64 complex vectors). There a warp per row leaves most of
+// the hop chain's latency exposed (a row's range, then its entries, then its
+// gathers, two 32-lane rounds for a 34-hop row), so here 8 lanes share a row
+// and a warp works on 4 rows at once; each lane takes every 8th hop of its
+// row with kRowU entries and gathers in flight, then the 8 partial sums are
+// folded by shuffles. The sum order differs from k_hv / k_hv_list (lane
+// partials over every 8th hop instead of every 32nd) but is fixed, so the
+// results are deterministic; the grid, and hence the order of the per-CTA
+// dot-product partials, is the other kernels'.
+constexpr int kRowLanes = 8;
+constexpr int kRowU = 4;
+
+template <typename W, typename T, int NV>
+__global__ void __launch_bounds__(kHvThreads, 4) k_hv_rows(const __grid_constant__ HvParams<W> P,
+                                                           const int64_t* __restrict__ hptr,
+                                                           const uint64_t* __restrict__ hops,
+                                                           const typename CT<T>::V* __restrict__ in,
+                                                           typename CT<T>::V* __restrict__ out,
+                                                           const double* __restrict__ scale,
+                                                           double* __restrict__ partial) {
+  using V = typename CT<T>::V;
+  constexpr int VPL = CT<T>::VPL;
+  static_assert(NV == VPL, "one 16-byte chunk per row");
+  constexpr int kRowsPerWarp = 32 / kRowLanes;
+  __shared__ double s_ph[2][64];
+  __shared__ double s_amp[2][8];
+  __shared__ double s_sq[65];
+  __shared__ double s_dot[kHvWarps][kRowsPerWarp][NV];
+  const Geom& g = P.g;
+  const BlockView<W>& v = P.v;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < 64; i += kHvThreads) {
+    s_ph[0][i] = v.phase_re[i];
+    s_ph[1][i] = v.phase_im[i];
+  }
+  if (tid < 8) {
+    s_amp[0][tid] = g.amp_re[tid];
+    s_amp[1][tid] = g.amp_im[tid];
+  }
+  if (tid < 65) s_sq[tid] = g.sqrt_deg[tid];
+  __syncthreads();
+  const int lane = tid & 31;
+  const int wid = tid >> 5;
+  const int grp = lane / kRowLanes;
+  const int sub = lane % kRowLanes;
+  double sc[VPL], dot[VPL];
+#pragma unroll
+  for (int e = 0; e < VPL; ++e) {
+    sc[e] = scale ? scale[e] : 1.0;
+    dot[e] = 0.0;
+  }
+  const int64_t nwarps = static_cast<int64_t>(gridDim.x) * kHvWarps;
+  // warp-uniform loop over groups of 4 rows (the shuffles need all lanes)
+  for (int64_t rb = (static_cast<int64_t>(blockIdx.x) * kHvWarps + wid) * kRowsPerWarp; rb < v.dim;
+       rb += nwarps * kRowsPerWarp) {
+    const int64_t row = rb + grp;
+    const bool ok = row < v.dim;
+    uint32_t meta = 0;
+    int64_t h0 = 0, h1 = 0;
+    if (ok) {
+      meta = __ldg(v.row_meta + row);
+      h0 = __ldg(hptr + row);
+      h1 = __ldg(hptr + row + 1);
+    }
+    const double inv_s = 1.0 / s_sq[static_cast<int>(meta >> 26) + 1];
+    V acc;
+    vzero(acc);
+    for (int64_t q0 = h0 + sub; q0 < h1; q0 += kRowLanes * kRowU) {
+      uint64_t e[kRowU];
+#pragma unroll
+      for (int u = 0; u < kRowU; ++u) {
+        const int64_t q = q0 + u * kRowLanes;
+        e[u] = q < h1 ? ld_stream_u64(hops + q) : ~0ULL;
+      }
+      V x[kRowU];
+      T cr[kRowU], ci[kRowU];
+#pragma unroll
+      for (int u = 0; u < kRowU; ++u) {
+        cr[u] = 0;
+        ci[u] = 0;
+        vzero(x[u]);
+        if (e[u] != ~0ULL) {
+          const int64_t col = static_cast<int64_t>(static_cast<uint32_t>(e[u]));
+          const int dir = static_cast<int>((e[u] >> 32) & 7);
+          const int p = static_cast<int>((e[u] >> 35) & 1);
+          const int shift = static_cast<int>((e[u] >> 36) & 63);
+          const int deg_t = static_cast<int>((e[u] >> 42) & 127);
+          const double ar = p ? -s_amp[0][dir] : s_amp[0][dir];
+          const double ai = p ? -s_amp[1][dir] : s_amp[1][dir];
+          const double pr = s_ph[0][shift], pi = s_ph[1][shift];
+          const double ratio = s_sq[deg_t] * inv_s;
+          cr[u] = static_cast<T>((ar * pr - ai * pi) * ratio);
+          ci[u] = static_cast<T>((ar * pi + ai * pr) * ratio);
+          x[u] = ld_stream(in + col);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kRowU; ++u) cfma<T>(acc, cr[u], ci[u], x[u]);
+    }
+#pragma unroll
+    for (int o = kRowLanes / 2; o > 0; o >>= 1) vadd(acc, shfl_xor_v(acc, o));
+    if (sub == 0 && ok) {
+      const W uw = __ldg(v.ur_bits + (meta & 0x3FFFFFFu));
+      const W dw = __ldg(v.row_dn + row);
+      const double diag = diag_energy(uw, dw, g);
+      const V xr = ld_stream(in + row);
+      out[row] = finish_row(xr, acc, diag, sc, dot);
+    }
+  }
+  if (partial) {
+    if (sub == 0) {
+#pragma unroll
+      for (int e = 0; e < VPL; ++e) s_dot[wid][grp][e] = dot[e];
+    }
+    __syncthreads();
+    for (int vv = tid; vv < NV; vv += kHvThreads) {
+      double s = 0.0;
+      for (int w = 0; w < kHvWarps; ++w)
+        for (int r = 0; r < kRowsPerWarp; ++r) s += s_dot[w][r][vv];
+      partial[static_cast<int64_t>(blockIdx.x) * NV + vv] = s;
+    }
+  }
+}
+
 template <typename W, typename R, typename T, int NV, int U, int MINB>
 void launch_hv_t(Ctx& c, const void* in, void* out, const double* scale, double* partial, int grid) {
   HvParams<W> P;
@@ -646,6 +771,14 @@ void launch_hv_t(Ctx& c, const void* in, void* out, const double* scale, double*
   else P.v = view64(c);
   using V = typename CT<T>::V;
   if (c.hl_active) {
+    if constexpr (NV == CT<T>::VPL) {
+      if (c.hv_rows) {
+        k_hv_rows<W, T, NV><<<grid, kHvThreads, 0, c.stream>>>(P, c.hl_ptr.as<int64_t>(), c.hl_ent.as<uint64_t>(),
+                                                               static_cast<const V*>(in), static_cast<V*>(out),
+                                                               scale, partial);
+        return;
+      }
+    }
     k_hv_list<W, T, NV, U, MINB><<<grid, kHvThreads, 0, c.stream>>>(P, c.hl_ptr.as<int64_t>(), c.hl_ent.as<uint64_t>(),
                                                                     static_cast<const V*>(in), static_cast<V*>(out),
                                                                     scale, partial);

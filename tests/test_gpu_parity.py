@@ -188,6 +188,7 @@ def test_cached_hop_list_equals_on_the_fly(golden, monkeypatch, prec, batch):
     m = model_of(golden, "c4x4")
     opts = pkg.RunOpts(samples=4, lanczos_steps=30, precision=prec, batch_vectors=batch,
                        start_vector=E.START_PHILOX_PHASE)
+    monkeypatch.setenv("FTLM_HV_ROWS", "0")  # the warp-per-row list kernel (same sum order)
     out = {}
     for mode in ("fly", "list"):
         monkeypatch.setenv("FTLM_HV_MODE", mode)
@@ -196,6 +197,29 @@ def test_cached_hop_list_equals_on_the_fly(golden, monkeypatch, prec, batch):
             out[mode] = eng.block_lanczos(1, 2)
     for a, b in zip(out["fly"], out["list"]):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("prec,batch,tol", [(E.PREC_FP64, 1, 1e-12), (E.PREC_MIXED, 2, 2e-5)])
+def test_narrow_sweep_row_kernel(golden, monkeypatch, prec, batch, tol):
+    """Sweeps of one 16-byte chunk per row on the hop list run 8 lanes per
+    row: same alpha/beta as the on-the-fly kernel up to rounding (another sum
+    order), deterministic from run to run."""
+    m = model_of(golden, "c4x4")
+    opts = pkg.RunOpts(samples=4, lanczos_steps=30, precision=prec, batch_vectors=batch,
+                       start_vector=E.START_PHILOX_PHASE)
+    out = {}
+    for key, mode in (("fly", "fly"), ("rows", "list"), ("rows2", "list")):
+        monkeypatch.setenv("FTLM_HV_MODE", mode)
+        with pkg.Engine(m, opts) as eng:
+            eng.sector_prepare(2, 3)
+            out[key] = eng.block_lanczos(1, 2)
+    for a, b in zip(out["rows"], out["rows2"]):
+        assert np.array_equal(a, b)
+    (af, bf, sf), (ar, br, sr) = out["fly"][:3], out["rows"][:3]
+    assert np.array_equal(sf, sr)
+    n = 10  # well before the reproducibility horizon
+    assert np.abs(ar[:, :n] - af[:, :n]).max() <= tol * np.abs(af[:, :n]).max()
+    assert np.abs(br[:, :n] - bf[:, :n]).max() <= tol * np.abs(bf[:, :n]).max()
 
 
 def test_exact_eigenvalues_match_reference(golden):
