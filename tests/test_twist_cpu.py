@@ -100,3 +100,26 @@ def test_block_features_periodicity():
     assert np.allclose(a, block_features(4.25, 2.5, 3, 4, 1, 0, 4, 2))
     assert not np.allclose(a, block_features(1.25, 0.5, 3, 4, 1, 0, 4, 2))
     assert sum(a[8:]) == 4.0 and a[8 + 3] == 1 and a[8 + 9 + 4] == 1 and a[8 + 18 + 1] == 1 and a[8 + 22] == 1
+
+
+def test_level_importance_is_a_boltzmann_probability():
+    """The loss weight of a level is the largest probability it reaches on
+    the (beta, mu) grid: in [0, 1], 1 for a level that alone dominates at some
+    mu, and tails count in the normalisation."""
+    from ftlm_extended_hubbard_development_b200.surrogate import level_importance
+    betas, mu = [2.0, 8.0], np.linspace(-3.0, 3.0, 61)
+    blocks = []
+    for p, e0 in ((0, 0.0), (1, -1.0), (2, 0.5)):
+        E = np.array([e0, e0 + 0.3, e0 + 2.0, 0.0])
+        W = np.array([1.0, 2.0, 1.0, 0.0])
+        M = np.array([1.0, 1.0, 1.0, 0.0])
+        blocks.append((0, 0, 0, 0, p, E, W, M, tail_log_partition(np.array([e0 + 3.0]), np.array([5.0]), betas)))
+    imp = level_importance(blocks, betas, mu)
+    assert imp.shape == (3, 4) and (imp >= 0).all() and (imp <= 1 + 1e-12).all()
+    assert imp[:, 3].max() == 0.0            # absent levels carry no weight
+    # deep inside a block's mu window at beta = 8 its ground level has
+    # probability 1 / (1 + 2 e^{-2.4} + e^{-16} + 5 e^{-24}) (own excited
+    # levels and tail; the other blocks are negligible there)
+    p0 = 1.0 / (1.0 + 2.0 * math.exp(-2.4) + math.exp(-16.0) + 5.0 * math.exp(-24.0))
+    assert np.allclose(imp[:, 0], p0, rtol=2e-3)
+    assert (imp[:, 2] < imp[:, 0]).all()     # higher levels matter less
