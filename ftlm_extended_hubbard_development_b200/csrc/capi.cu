@@ -16,6 +16,10 @@ struct ftlm_ctx {
 };
 
 namespace ftlm {
+
+// Never launched: its attributes tell which code object the runtime loaded.
+__global__ void k_code_probe() {}
+
 namespace {
 
 const double kPi = 3.141592653589793238462643383279502884;
@@ -114,6 +118,29 @@ extern "C" {
 
 int ftlm_abi_version(void) { return FTLM_ABI_VERSION; }
 
+int ftlm_device_code_version(int32_t device, int32_t* binary_version, int32_t* ptx_version) {
+  if (!binary_version || !ptx_version) return FTLM_ERR_ARG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+    cudaGetLastError();
+    return FTLM_ERR_CUDA;
+  }
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaFuncAttributes a{};
+  const cudaError_t e = cudaSetDevice(device) == cudaSuccess
+                            ? cudaFuncGetAttributes(&a, reinterpret_cast<const void*>(ftlm::k_code_probe))
+                            : cudaErrorInvalidDevice;
+  cudaSetDevice(prev);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return FTLM_ERR_CUDA;
+  }
+  *binary_version = a.binaryVersion;
+  *ptx_version = a.ptxVersion;
+  return FTLM_OK;
+}
+
 int ftlm_ctx_create(const ftlm_model* model, const ftlm_run_opts* opts, ftlm_ctx** out) {
   if (!model || !opts || !out) return FTLM_ERR_ARG;
   *out = nullptr;
@@ -132,8 +159,11 @@ int ftlm_ctx_create(const ftlm_model* model, const ftlm_run_opts* opts, ftlm_ctx
   c.device = opts->device;
   c.wide = model->lx * model->ly > 32;
   if (const char* hv = std::getenv("FTLM_HV_VARIANT")) c.hv_forced = std::atoi(hv);
-  if (const char* hm = std::getenv("FTLM_HV_MODE"))
-    c.hv_mode = std::string(hm) == "list" ? 1 : (std::string(hm) == "fly" ? 0 : -1);
+  if (const char* rt = std::getenv("FTLM_HV_RETUNE")) c.hv_retune = std::string(rt) == "1";
+  if (const char* hm = std::getenv("FTLM_HV_MODE")) {
+    const std::string m(hm);
+    c.hv_mode = m == "list" ? ftlm::kSrcList : m == "fly" ? ftlm::kSrcFly : m == "split" ? ftlm::kSrcSplit : -1;
+  }
   if (const char* sb = std::getenv("FTLM_SMALL_BLOCKS")) c.small_blocks = std::string(sb) != "0";
   if (const char* hr = std::getenv("FTLM_HV_ROWS")) c.hv_rows = std::string(hr) != "0";
   int ndev = 0;
@@ -169,8 +199,17 @@ void ftlm_ctx_destroy(ftlm_ctx* ctx) {
                         &c.lz_alpha, &c.lz_beta, &c.lz_scale, &c.lz_state, &c.host_start, &c.ritz_tmp, &c.ritz_out, &c.ritz_meta,
                         &c.sb_rp, &c.sb_col, &c.sb_val, &c.sb_diag, &c.sb_meta, &c.sb_steps,
                         &c.scan_tmp, &c.dense_arena, &c.dense_meta, &c.dense_out, &c.spectra, &c.th_beta,
-                        &c.th_mu, &c.th_state, &c.hl_ptr, &c.hl_ent};
+                        &c.th_mu, &c.th_state, &c.hl_ptr, &c.hl_ent, &c.flip_map, &c.vec_xd, &c.vec_yd};
   for (auto* b : bufs) b->release();
+  if (c.flipped) {
+    ftlm::Ctx& f = *c.flipped;
+    ftlm::DBuf* fb[] = {&f.sec.ups, &f.sec.dns, &f.sec.up_info, &f.sec.ur_bits, &f.sec.ur_class, &f.sec.ur_poff,
+                        &f.sec.d_star, &f.sec.d_hs, &f.sec.d_stab, &f.sec.d_chi, &f.sec.d_cidx, &f.sec.canon,
+                        &f.sec.tmp_a, &f.sec.tmp_b, &f.sec.tmp_c, &f.sec.tmp_d, &f.sec.tmp_e, &f.blk.act,
+                        &f.blk.act_list, &f.blk.aoff, &f.blk.dtab, &f.blk.row_meta, &f.blk.row_dn, &f.scan_tmp};
+    for (auto* b : fb) b->release();  // binom tables are the owner's
+    c.flipped.reset();
+  }
   if (c.stream) cudaStreamDestroy(c.stream);
   delete ctx;
 }
@@ -397,13 +436,21 @@ int ftlm_block_apply(ftlm_ctx* ctx, int32_t mx, int32_t my, int32_t nvec, const 
       }
     FTLM_CUDA(cudaMemcpyAsync(c.vec_a.p, h.data(), bytes, cudaMemcpyHostToDevice, c.stream));
     c.prof.h2d_bytes += static_cast<int64_t>(bytes);
+    ftlm::HvSourceGuard guard{c};
+    c.prof.hv_source = ftlm::hv_select_source(c, NV, fp32);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (c.timing) {
       FTLM_CUDA(cudaEventCreate(&e0));
       FTLM_CUDA(cudaEventCreate(&e1));
       FTLM_CUDA(cudaEventRecord(e0, c.stream));
     }
-    ftlm::hv_apply(c, c.vec_a.p, c.vec_h.p, NV, fp32, nullptr, nullptr, 0);
+    if (c.split_active) {
+      ftlm::flip_scatter(c, c.vec_a.p, c.vec_xd.p, NV, fp32);
+      ftlm::hv_apply_split(c, c.vec_a.p, c.vec_xd.p, c.vec_h.p, c.vec_yd.p, NV, fp32, nullptr, nullptr);
+      ftlm::flip_gather_add(c, c.vec_h.p, c.vec_yd.p, NV, fp32);
+    } else {
+      ftlm::hv_apply(c, c.vec_a.p, c.vec_h.p, NV, fp32, nullptr, nullptr, 0);
+    }
     if (c.timing) {
       FTLM_CUDA(cudaEventRecord(e1, c.stream));
     }
@@ -420,6 +467,8 @@ int ftlm_block_apply(ftlm_ctx* ctx, int32_t mx, int32_t my, int32_t nvec, const 
       const double s = fp32 ? 8.0 : 16.0;
       const double nzh = static_cast<double>(ftlm::block_nonzero_hops(c));
       c.prof.hv_bytes += static_cast<double>(D) * nvec * s * 2.0 + nzh * nvec * s + static_cast<double>(D) * 8.0;
+      c.prof.hv_hops += nzh * nvec;
+      c.prof.hv_min_bytes += static_cast<double>(D) * (2.0 * nvec * s + 8.0);
     }
     for (int64_t i = 0; i < D; ++i)
       for (int v = 0; v < nvec; ++v) {
@@ -524,6 +573,10 @@ int ftlm_profile_read(ftlm_ctx* ctx, ftlm_profile* out) {
     out->tune_runs = p.tune_runs;
     out->small_ms = p.small_ms;
     out->small_tasks = p.small_tasks;
+    out->hv_hops = p.hv_hops;
+    out->hv_min_bytes = p.hv_min_bytes;
+    out->hv_source = p.hv_source;
+    out->pad0 = 0;
   });
 }
 

@@ -167,6 +167,26 @@ __device__ W unrank(uint64_t r, int k, int n, const uint64_t* binom) {
   return x;
 }
 
+// Exact fixed-point accumulation of FP64 terms (the Lanczos dot products):
+// v -> round(v * 2^64) as a 128-bit two's-complement integer. Integer sums
+// are associative, so a sum of converted terms does not depend on the order
+// or grouping of its terms (grid size, row scheduling, kernel variant).
+// Terms and sums must stay below 2^62 in magnitude; resolution 2^-64.
+typedef unsigned __int128 fx128;
+
+__device__ __forceinline__ fx128 fx_of(double v) {
+  const double h = floor(v);
+  const double l = v - h;  // exact, 0 <= l < 1
+  const unsigned long long hi = static_cast<unsigned long long>(static_cast<long long>(h));
+  return (static_cast<fx128>(hi) << 64) + static_cast<fx128>(__double2ull_rn(l * 18446744073709551616.0));
+}
+
+__device__ __forceinline__ double fx_to_double(fx128 a) {
+  const long long hi = static_cast<long long>(static_cast<unsigned long long>(a >> 64));
+  const unsigned long long lo = static_cast<unsigned long long>(a);
+  return static_cast<double>(hi) + static_cast<double>(lo) * 5.42101086242752217003726400434970855712890625e-20;
+}
+
 // Philox4x32-10 counter-based generator (Salmon, Moraes, Dror, Shaw, SC'11).
 struct P4 {
   uint32_t x[4];

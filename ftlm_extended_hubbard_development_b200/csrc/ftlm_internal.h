@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <map>
+#include <memory>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -155,6 +156,14 @@ struct Profile {
   int tune_runs = 0;    // autotuner measurements made by this context
   double small_ms = 0.0;     // device time of small-block Lanczos launches
   int64_t small_tasks = 0;   // (block, random vector) pairs they ran
+  double hv_hops = 0.0;      // nonzero hop x vector products of the timed H*V launches
+  double hv_min_bytes = 0.0; // their compulsory bytes D * (2 nv s + 8) per launch
+  int hv_source = -1;        // operator source of the last sweep (kSrcFly / kSrcList / kSrcSplit)
+};
+
+// Momentum phases e^{i k.s} of a block, by translation index s.
+struct FlipPhase {
+  double re[64], im[64];
 };
 
 // Largest block dimension the small-block Lanczos launch takes (three FP64
@@ -167,8 +176,17 @@ struct Ctx {
   Geom geom{};
   bool wide = false;  // 64-bit spin words (more than 32 sites)
   int hv_forced = -1; // H*V kernel variant forced by FTLM_HV_VARIANT (-1: autotune)
-  int hv_mode = -1;   // H*V operator source: -1 auto, 0 on-the-fly lookups, 1 cached hop list (FTLM_HV_MODE)
+  bool hv_retune = false;  // FTLM_HV_RETUNE=1: tune once per context, ignoring the process-wide choices
+  std::map<uint64_t, int> tuned_local;  // variants chosen by this context's tuner runs
+  int hv_mode = -1;   // H*V operator source: -1 auto, 0 on-the-fly lookups, 1 cached hop list,
+                      // 2 split-spin segment sweeps (FTLM_HV_MODE=fly|list|split)
   bool hl_active = false;  // H*V kernels read the cached hop list of the prepared block
+  bool split_active = false;  // H*V runs as the two segment sweeps of split.cu
+  std::unique_ptr<Ctx> flipped;  // tables of sector (N_down, N_up) when N_up != N_down
+  DBuf flip_map;      // uint64 per row: flipped row | shift << 32 | sign << 38 (+ an error word)
+  int flip_for[4] = {-1, -1, -1, -1};  // (n_up, n_dn, mx, my) the flip map belongs to
+  int64_t flip_gen = -1, sec_gen = 0;  // sector generation of the flip map / of the tables
+  DBuf vec_xd, vec_yd;  // Lanczos vector and H*V output in the spin-flipped row order
   bool hv_rows = true;  // narrow sweeps on the hop list: 8 lanes per row (FTLM_HV_ROWS=0: warp per row)
   bool small_blocks = true;  // batched FTLM runs blocks <= kSmallMaxDim in one launch (FTLM_SMALL_BLOCKS=0: off)
   int64_t hl_nnz = 0;
@@ -218,9 +236,46 @@ int64_t block_csr_device(Ctx& c, DBuf& row_ptr, DBuf& col, DBuf& val, DBuf& diag
 // caller), entries summed in the CSR's order; no host synchronisation.
 void block_dense_device(Ctx& c, double2* A);
 // H*V of the prepared block on device arrays [dim][nv] complex (FP64 or FP32).
+// partial_dev[grid][nv] receives each CTA's fixed-point sum of Re<s x, y>.
 void hv_apply(Ctx& c, const void* in, void* out, int nv, bool fp32, const double* scale_dev,
-              double* partial_dev, int nblocks_hint);
+              fx128* partial_dev, int nblocks_hint);
 int hv_grid(Ctx& c, int nv, bool fp32);
+// Chooses the operator source of sweeps of nv vectors over the prepared
+// block (FTLM_HV_MODE or the automatic rule): on-the-fly lookups, the cached
+// hop list (few vectors per sweep), or the split-spin segment sweeps (large
+// blocks); builds what it needs and sets c.hl_active / c.split_active. The
+// guard clears them again.
+enum { kSrcFly = 0, kSrcList = 1, kSrcSplit = 2 };
+constexpr int64_t kSplitMinDim = int64_t(1) << 15;
+int hv_select_source(Ctx& c, int nv, bool fp32);
+struct HvSourceGuard {
+  Ctx& c;
+  ~HvSourceGuard() {
+    c.hl_active = false;
+    c.split_active = false;
+  }
+};
+// Autotuner cache (hv.cu): variant chosen for a key by this context or the process.
+int hv_size_class(int64_t dim);
+bool hv_tuned_lookup(Ctx& c, uint64_t key, int& var);
+void hv_tuned_store(Ctx& c, uint64_t key, int var);
+
+// ---- split-spin H*V (split.cu)
+// Prepares the spin-flipped tables and the flip map of the prepared block and
+// the two flipped-order arrays for sweeps of nv vectors; false when they do
+// not fit in device memory.
+bool split_prepare(Ctx& c, int nv, bool fp32);
+// y = M x for x given in both row orders: out (this block's order, diagonal
+// included) and out_d (flipped order) such that M x = out + S^T out_d.
+// partial receives 2 x grid rows of fixed-point Re<s x, y> sums; returns
+// that row count.
+int hv_apply_split(Ctx& c, const void* in, const void* in_d, void* out, void* out_d, int nv, bool fp32,
+                   const double* scale, fx128* partial);
+int hv_split_max_grid(const Ctx& c);
+// x_D[p(q)] = conj(f_q) x[q];  y[q] += f_q y_D[p(q)].
+void flip_scatter(Ctx& c, const void* x, void* xd, int nv, bool fp32);
+void flip_gather_add(Ctx& c, void* y, const void* yd, int nv, bool fp32);
+FlipPhase flip_phase(const Ctx& c);
 BlockView<uint32_t> view32(Ctx& c);
 BlockView<uint64_t> view64(Ctx& c);
 

@@ -20,6 +20,7 @@
 #include <tuple>
 
 #include "ftlm_internal.h"
+#include "hv_common.cuh"
 
 namespace ftlm {
 
@@ -27,48 +28,6 @@ namespace {
 
 int grid_for(int64_t n, int threads) {
   return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>((n + threads - 1) / threads, 1 << 20)));
-}
-
-// Resolve a hop target (tu, td) to its block column, translation shift,
-// sign parity and orbit stabiliser size. Returns false when the target's
-// orbit is inactive in this block (main.cpp:790-793).
-template <typename W, typename R>
-__device__ __forceinline__ bool resolve(W tu, W td, bool up_hop, uint32_t ur_src, const BlockView<W>& v,
-                                        const Geom& g, const R* binom, int64_t& col, int& shift, int& sgn,
-                                        int& deg) {
-  uint32_t ur = ur_src;
-  int g0 = 0;
-  int s = 0;
-  W dd = td;
-  if (up_hop) {
-    const uint64_t info = __ldg(v.up_info + rank_of<W, R>(tu, binom));
-    ur = static_cast<uint32_t>(info);
-    g0 = static_cast<int>((info >> 32) & 0xFF);
-    s = static_cast<int>((info >> 40) & 1);
-    if (g0) {
-      int p;
-      const int ng = shift_neg(g0, g);
-      dd = translate(td, shift_dx(ng, g), shift_dy(ng, g), g, &p);
-      s ^= p;
-    }
-  }
-  const int cls = __ldg(v.ur_class + ur);
-  const int64_t rd = static_cast<int64_t>(rank_of<W, R>(dd, binom));
-  int64_t a = rd;
-  int h = 0;
-  deg = 1;
-  if (cls != 0) {
-    const uint64_t e = __ldg(v.dtab + static_cast<int64_t>(cls - 1) * v.c_dn + rd);
-    a = static_cast<int32_t>(static_cast<uint32_t>(e));
-    if (a < 0) return false;
-    h = static_cast<int>((e >> 32) & 0xFF);
-    s ^= static_cast<int>((e >> 40) & 1);
-    deg = static_cast<int>((e >> 48) & 0xFF);
-  }
-  shift = h ? shift_add(g0, h, g) : g0;
-  sgn = s;
-  col = __ldg(v.aoff + ur) + a;
-  return true;
 }
 
 template <typename W>
@@ -153,171 +112,6 @@ __global__ void k_i64_to_i32(const int64_t* __restrict__ in, int32_t* __restrict
 
 // ------------------------------------------------------------ H*V kernel
 
-template <typename T>
-struct CT;  // 16-byte chunk type and complex-per-chunk count
-template <>
-struct CT<float> {
-  using V = float4;
-  static constexpr int VPL = 2;
-};
-template <>
-struct CT<double> {
-  using V = double2;
-  static constexpr int VPL = 1;
-};
-
-template <typename W>
-struct HvParams {
-  Geom g;
-  BlockView<W> v;
-};
-
-constexpr int kHvThreads = 256;
-constexpr int kHvWarps = kHvThreads / 32;
-// hop codes per warp: 8 directions * (N_up + N_down) <= 16 * bits per word
-template <typename W>
-constexpr int queue_len() { return 16 * static_cast<int>(sizeof(W)) * 8; }
-
-// k-th (0-based) set bit of x.
-template <typename W>
-__device__ __forceinline__ int kth_bit(W x, int k) {
-  int pos = 0;
-#pragma unroll
-  for (int w = sizeof(W) * 4; w >= 1; w >>= 1) {
-    const W lowmask = static_cast<W>((static_cast<W>(1) << w) - 1);
-    const int c = popc(static_cast<W>(x & lowmask));
-    if (k >= c) {
-      k -= c;
-      x >>= w;
-      pos += w;
-    }
-  }
-  return pos;
-}
-
-// Gathered vector rows stream through without allocating in L1, so the small
-// orbit tables of the target lookups (up_info, class tables, offsets) stay
-// L1-resident; L2 still caches the rows.
-__device__ __forceinline__ float4 ld_stream(const float4* p) {
-  float4 r;
-  asm("ld.global.nc.L1::no_allocate.v4.f32 {%0, %1, %2, %3}, [%4];"
-      : "=f"(r.x), "=f"(r.y), "=f"(r.z), "=f"(r.w)
-      : "l"(p));
-  return r;
-}
-__device__ __forceinline__ double2 ld_stream(const double2* p) {
-  double2 r;
-  asm("ld.global.nc.L1::no_allocate.v2.f64 {%0, %1}, [%2];" : "=d"(r.x), "=d"(r.y) : "l"(p));
-  return r;
-}
-
-template <typename T>
-__device__ __forceinline__ void cfma(typename CT<T>::V& acc, T cr, T ci, const typename CT<T>::V& x);
-
-template <>
-__device__ __forceinline__ void cfma<float>(float4& acc, float cr, float ci, const float4& x) {
-  acc.x = fmaf(cr, x.x, fmaf(-ci, x.y, acc.x));
-  acc.y = fmaf(cr, x.y, fmaf(ci, x.x, acc.y));
-  acc.z = fmaf(cr, x.z, fmaf(-ci, x.w, acc.z));
-  acc.w = fmaf(cr, x.w, fmaf(ci, x.z, acc.w));
-}
-template <>
-__device__ __forceinline__ void cfma<double>(double2& acc, double cr, double ci, const double2& x) {
-  acc.x = fma(cr, x.x, fma(-ci, x.y, acc.x));
-  acc.y = fma(cr, x.y, fma(ci, x.x, acc.y));
-}
-
-__device__ __forceinline__ float4 shfl_xor_v(float4 a, int m) {
-  a.x = __shfl_xor_sync(0xffffffffu, a.x, m);
-  a.y = __shfl_xor_sync(0xffffffffu, a.y, m);
-  a.z = __shfl_xor_sync(0xffffffffu, a.z, m);
-  a.w = __shfl_xor_sync(0xffffffffu, a.w, m);
-  return a;
-}
-__device__ __forceinline__ double2 shfl_xor_v(double2 a, int m) {
-  a.x = __shfl_xor_sync(0xffffffffu, a.x, m);
-  a.y = __shfl_xor_sync(0xffffffffu, a.y, m);
-  return a;
-}
-__device__ __forceinline__ void vzero(float4& a) { a = make_float4(0.f, 0.f, 0.f, 0.f); }
-__device__ __forceinline__ void vzero(double2& a) { a = make_double2(0.0, 0.0); }
-__device__ __forceinline__ void vadd(float4& a, const float4& b) {
-  a.x += b.x; a.y += b.y; a.z += b.z; a.w += b.w;
-}
-__device__ __forceinline__ void vadd(double2& a, const double2& b) {
-  a.x += b.x; a.y += b.y;
-}
-
-// y = s_v * (diag * x + acc) per complex element; returns Re(conj(s_v x) y)
-// summed per element into dot[e].
-__device__ __forceinline__ float4 finish_row(const float4& x, const float4& acc, double diag, const double* s,
-                                             double* dot) {
-  const float df = static_cast<float>(diag);
-  float4 y;
-  y.x = fmaf(df, x.x, acc.x);
-  y.y = fmaf(df, x.y, acc.y);
-  y.z = fmaf(df, x.z, acc.z);
-  y.w = fmaf(df, x.w, acc.w);
-  y.x = static_cast<float>(s[0] * y.x);
-  y.y = static_cast<float>(s[0] * y.y);
-  y.z = static_cast<float>(s[1] * y.z);
-  y.w = static_cast<float>(s[1] * y.w);
-  dot[0] += s[0] * (static_cast<double>(x.x) * y.x + static_cast<double>(x.y) * y.y);
-  dot[1] += s[1] * (static_cast<double>(x.z) * y.z + static_cast<double>(x.w) * y.w);
-  return y;
-}
-__device__ __forceinline__ double2 finish_row(const double2& x, const double2& acc, double diag, const double* s,
-                                              double* dot) {
-  double2 y;
-  y.x = s[0] * fma(diag, x.x, acc.x);
-  y.y = s[0] * fma(diag, x.y, acc.y);
-  dot[0] += s[0] * (x.x * y.x + x.y * y.y);
-  return y;
-}
-
-// Gathers of one batch of nb <= 32 hops, whose (column, coefficient) lane
-// q holds for hop q: groups of G lanes take hops grp, grp+HPAR, ..., U hops
-// per group per iteration with all their loads issued before any FMA
-// (U*LPL 16-byte gathers in flight per lane). Summation order per lane is
-// the hop order, independent of U.
-template <typename T, int NV, int U>
-__device__ __forceinline__ void gather_batch(const typename CT<T>::V* __restrict__ in, int64_t col, T cr, T ci,
-                                             int nb,
-                                             typename CT<T>::V (&acc)[(NV / CT<T>::VPL < 32 ? 1 : NV / CT<T>::VPL / 32)]) {
-  using V = typename CT<T>::V;
-  constexpr int CPR = NV / CT<T>::VPL;
-  constexpr int G = CPR < 32 ? CPR : 32;
-  constexpr int LPL = CPR / G;
-  constexpr int HPAR = 32 / G;
-  const int lane = threadIdx.x & 31;
-  const int grp = lane / G;
-  const int sub = lane % G;
-  for (int j = 0; j < nb; j += HPAR * U) {
-    int64_t c[U];
-    T r[U], i[U];
-    V x[U][LPL];
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int q = j + u * HPAR + grp;
-      c[u] = __shfl_sync(0xffffffffu, col, q & 31);
-      r[u] = __shfl_sync(0xffffffffu, cr, q & 31);
-      i[u] = __shfl_sync(0xffffffffu, ci, q & 31);
-      if (q >= nb) c[u] = -1;
-    }
-#pragma unroll
-    for (int u = 0; u < U; ++u)
-#pragma unroll
-      for (int l = 0; l < LPL; ++l) {
-        if (c[u] >= 0) x[u][l] = ld_stream(in + c[u] * CPR + l * G + sub);
-        else vzero(x[u][l]);
-      }
-#pragma unroll
-    for (int u = 0; u < U; ++u)
-#pragma unroll
-      for (int l = 0; l < LPL; ++l) cfma<T>(acc[l], r[u], i[u], x[u][l]);
-  }
-}
-
 // H*V over all rows of the block. in/out: [dim][NV] complex T as 16-byte
 // chunks. scale[v] multiplies the result of vector v (Lanczos vectors are
 // stored unnormalised). partial[block][NV] receives Re<s*in, out> sums
@@ -328,7 +122,7 @@ template <typename W, typename R, typename T, int NV, int U, int MINB>
 __global__ void __launch_bounds__(kHvThreads, MINB) k_hv(const __grid_constant__ HvParams<W> P,
                                                    const typename CT<T>::V* __restrict__ in,
                                                    typename CT<T>::V* __restrict__ out,
-                                                   const double* __restrict__ scale, double* __restrict__ partial,
+                                                   const double* __restrict__ scale, fx128* __restrict__ partial,
                                                    const R* __restrict__ gbinom) {
   using V = typename CT<T>::V;
   constexpr int VPL = CT<T>::VPL;
@@ -344,7 +138,7 @@ __global__ void __launch_bounds__(kHvThreads, MINB) k_hv(const __grid_constant__
   __shared__ double s_amp[2][8];
   __shared__ double s_sq[65];
   __shared__ uint16_t s_q[kHvWarps][kQ];
-  __shared__ double s_dot[kHvWarps][NV];
+  __shared__ fx128 s_acc[kHvWarps][NV];
 
   const Geom& g = P.g;
   const BlockView<W>& v = P.v;
@@ -362,6 +156,7 @@ __global__ void __launch_bounds__(kHvThreads, MINB) k_hv(const __grid_constant__
     s_amp[1][tid] = g.amp_im[tid];
   }
   if (tid < 65) s_sq[tid] = g.sqrt_deg[tid];
+  for (int i = tid; i < kHvWarps * NV; i += kHvThreads) s_acc[i / NV][i % NV] = 0;
   __syncthreads();
 
   const int lane = tid & 31;
@@ -371,14 +166,10 @@ __global__ void __launch_bounds__(kHvThreads, MINB) k_hv(const __grid_constant__
   uint16_t* queue = s_q[wid];
 
   double sc[LPL][VPL];
-  double dot[LPL][VPL];
 #pragma unroll
   for (int l = 0; l < LPL; ++l)
 #pragma unroll
-    for (int e = 0; e < VPL; ++e) {
-      sc[l][e] = scale ? scale[(l * G + sub) * VPL + e] : 1.0;
-      dot[l][e] = 0.0;
-    }
+    for (int e = 0; e < VPL; ++e) sc[l][e] = scale ? scale[(l * G + sub) * VPL + e] : 1.0;
 
   const int nsite = v.n_up + v.n_dn;
   const int64_t nwarps = static_cast<int64_t>(gridDim.x) * kHvWarps;
@@ -460,25 +251,16 @@ __global__ void __launch_bounds__(kHvThreads, MINB) k_hv(const __grid_constant__
 #pragma unroll
       for (int l = 0; l < LPL; ++l) {
         const V x = ld_stream(in + row * CPR + l * G + sub);
-        out[row * CPR + l * G + sub] = finish_row(x, acc[l], diag, sc[l], dot[l]);
+        double dt[VPL];
+        out[row * CPR + l * G + sub] = finish_row(x, acc[l], diag, sc[l], dt);
+        if (partial) {
+#pragma unroll
+          for (int e = 0; e < VPL; ++e) s_acc[wid][(l * G + sub) * VPL + e] += fx_of(dt[e]);
+        }
       }
     }
   }
-
-  if (partial) {
-    if (grp == 0) {
-#pragma unroll
-      for (int l = 0; l < LPL; ++l)
-#pragma unroll
-        for (int e = 0; e < VPL; ++e) s_dot[wid][(l * G + sub) * VPL + e] = dot[l][e];
-    }
-    __syncthreads();
-    for (int vv = tid; vv < NV; vv += kHvThreads) {
-      double s = 0.0;
-      for (int w = 0; w < kHvWarps; ++w) s += s_dot[w][vv];
-      partial[static_cast<int64_t>(blockIdx.x) * NV + vv] = s;
-    }
-  }
+  flush_dot<NV>(s_acc, partial);
 }
 
 // ------------------------------------------------------- cached hop list
@@ -543,7 +325,7 @@ __global__ void __launch_bounds__(kHvThreads, MINB) k_hv_list(const __grid_const
                                                               const typename CT<T>::V* __restrict__ in,
                                                               typename CT<T>::V* __restrict__ out,
                                                               const double* __restrict__ scale,
-                                                              double* __restrict__ partial) {
+                                                              fx128* __restrict__ partial) {
   using V = typename CT<T>::V;
   constexpr int VPL = CT<T>::VPL;
   constexpr int CPR = NV / VPL;
@@ -552,7 +334,7 @@ __global__ void __launch_bounds__(kHvThreads, MINB) k_hv_list(const __grid_const
   __shared__ double s_ph[2][64];
   __shared__ double s_amp[2][8];
   __shared__ double s_sq[65];
-  __shared__ double s_dot[kHvWarps][NV];
+  __shared__ fx128 s_acc[kHvWarps][NV];
   const Geom& g = P.g;
   const BlockView<W>& v = P.v;
   const int tid = threadIdx.x;
@@ -565,20 +347,17 @@ __global__ void __launch_bounds__(kHvThreads, MINB) k_hv_list(const __grid_const
     s_amp[1][tid] = g.amp_im[tid];
   }
   if (tid < 65) s_sq[tid] = g.sqrt_deg[tid];
+  for (int i = tid; i < kHvWarps * NV; i += kHvThreads) s_acc[i / NV][i % NV] = 0;
   __syncthreads();
   const int lane = tid & 31;
   const int wid = tid >> 5;
   const int grp = lane / G;
   const int sub = lane % G;
   double sc[LPL][VPL];
-  double dot[LPL][VPL];
 #pragma unroll
   for (int l = 0; l < LPL; ++l)
 #pragma unroll
-    for (int e = 0; e < VPL; ++e) {
-      sc[l][e] = scale ? scale[(l * G + sub) * VPL + e] : 1.0;
-      dot[l][e] = 0.0;
-    }
+    for (int e = 0; e < VPL; ++e) sc[l][e] = scale ? scale[(l * G + sub) * VPL + e] : 1.0;
   const int64_t nwarps = static_cast<int64_t>(gridDim.x) * kHvWarps;
   for (int64_t row = static_cast<int64_t>(blockIdx.x) * kHvWarps + wid; row < v.dim; row += nwarps) {
     const uint32_t meta = __ldg(v.row_meta + row);
@@ -618,24 +397,16 @@ __global__ void __launch_bounds__(kHvThreads, MINB) k_hv_list(const __grid_const
 #pragma unroll
       for (int l = 0; l < LPL; ++l) {
         const V x = ld_stream(in + row * CPR + l * G + sub);
-        out[row * CPR + l * G + sub] = finish_row(x, acc[l], diag, sc[l], dot[l]);
+        double dt[VPL];
+        out[row * CPR + l * G + sub] = finish_row(x, acc[l], diag, sc[l], dt);
+        if (partial) {
+#pragma unroll
+          for (int e = 0; e < VPL; ++e) s_acc[wid][(l * G + sub) * VPL + e] += fx_of(dt[e]);
+        }
       }
     }
   }
-  if (partial) {
-    if (grp == 0) {
-#pragma unroll
-      for (int l = 0; l < LPL; ++l)
-#pragma unroll
-        for (int e = 0; e < VPL; ++e) s_dot[wid][(l * G + sub) * VPL + e] = dot[l][e];
-    }
-    __syncthreads();
-    for (int vv = tid; vv < NV; vv += kHvThreads) {
-      double s = 0.0;
-      for (int w = 0; w < kHvWarps; ++w) s += s_dot[w][vv];
-      partial[static_cast<int64_t>(blockIdx.x) * NV + vv] = s;
-    }
-  }
+  flush_dot<NV>(s_acc, partial);
 }
 
 // H*V from the cached hop list for sweeps whose row is one 16-byte chunk
@@ -658,7 +429,7 @@ __global__ void __launch_bounds__(kHvThreads, 4) k_hv_rows(const __grid_constant
                                                            const typename CT<T>::V* __restrict__ in,
                                                            typename CT<T>::V* __restrict__ out,
                                                            const double* __restrict__ scale,
-                                                           double* __restrict__ partial) {
+                                                           fx128* __restrict__ partial) {
   using V = typename CT<T>::V;
   constexpr int VPL = CT<T>::VPL;
   static_assert(NV == VPL, "one 16-byte chunk per row");
@@ -666,7 +437,7 @@ __global__ void __launch_bounds__(kHvThreads, 4) k_hv_rows(const __grid_constant
   __shared__ double s_ph[2][64];
   __shared__ double s_amp[2][8];
   __shared__ double s_sq[65];
-  __shared__ double s_dot[kHvWarps][kRowsPerWarp][NV];
+  __shared__ fx128 s_acc[kHvWarps * kRowsPerWarp][NV];
   const Geom& g = P.g;
   const BlockView<W>& v = P.v;
   const int tid = threadIdx.x;
@@ -679,17 +450,15 @@ __global__ void __launch_bounds__(kHvThreads, 4) k_hv_rows(const __grid_constant
     s_amp[1][tid] = g.amp_im[tid];
   }
   if (tid < 65) s_sq[tid] = g.sqrt_deg[tid];
+  for (int i = tid; i < kHvWarps * kRowsPerWarp * NV; i += kHvThreads) s_acc[i / NV][i % NV] = 0;
   __syncthreads();
   const int lane = tid & 31;
   const int wid = tid >> 5;
   const int grp = lane / kRowLanes;
   const int sub = lane % kRowLanes;
-  double sc[VPL], dot[VPL];
+  double sc[VPL];
 #pragma unroll
-  for (int e = 0; e < VPL; ++e) {
-    sc[e] = scale ? scale[e] : 1.0;
-    dot[e] = 0.0;
-  }
+  for (int e = 0; e < VPL; ++e) sc[e] = scale ? scale[e] : 1.0;
   const int64_t nwarps = static_cast<int64_t>(gridDim.x) * kHvWarps;
   // warp-uniform loop over groups of 4 rows (the shuffles need all lanes)
   for (int64_t rb = (static_cast<int64_t>(blockIdx.x) * kHvWarps + wid) * kRowsPerWarp; rb < v.dim;
@@ -745,26 +514,19 @@ __global__ void __launch_bounds__(kHvThreads, 4) k_hv_rows(const __grid_constant
       const W dw = __ldg(v.row_dn + row);
       const double diag = diag_energy(uw, dw, g);
       const V xr = ld_stream(in + row);
-      out[row] = finish_row(xr, acc, diag, sc, dot);
-    }
-  }
-  if (partial) {
-    if (sub == 0) {
+      double dt[VPL];
+      out[row] = finish_row(xr, acc, diag, sc, dt);
+      if (partial) {
 #pragma unroll
-      for (int e = 0; e < VPL; ++e) s_dot[wid][grp][e] = dot[e];
-    }
-    __syncthreads();
-    for (int vv = tid; vv < NV; vv += kHvThreads) {
-      double s = 0.0;
-      for (int w = 0; w < kHvWarps; ++w)
-        for (int r = 0; r < kRowsPerWarp; ++r) s += s_dot[w][r][vv];
-      partial[static_cast<int64_t>(blockIdx.x) * NV + vv] = s;
+        for (int e = 0; e < VPL; ++e) s_acc[wid * kRowsPerWarp + grp][e] += fx_of(dt[e]);
+      }
     }
   }
+  flush_dot<NV>(s_acc, partial);
 }
 
 template <typename W, typename R, typename T, int NV, int U, int MINB>
-void launch_hv_t(Ctx& c, const void* in, void* out, const double* scale, double* partial, int grid) {
+void launch_hv_t(Ctx& c, const void* in, void* out, const double* scale, fx128* partial, int grid) {
   HvParams<W> P;
   P.g = c.geom;
   if constexpr (sizeof(W) == 4) P.v = view32(c);
@@ -794,7 +556,7 @@ void launch_hv_t(Ctx& c, const void* in, void* out, const double* scale, double*
 constexpr int kNumVariants = 5;
 
 template <typename W, typename R, typename T, int NV>
-void launch_hv_var(Ctx& c, int var, const void* in, void* out, const double* scale, double* partial, int grid) {
+void launch_hv_var(Ctx& c, int var, const void* in, void* out, const double* scale, fx128* partial, int grid) {
   switch (var) {
     case 0: launch_hv_t<W, R, T, NV, 1, 4>(c, in, out, scale, partial, grid); return;
     case 1: launch_hv_t<W, R, T, NV, 2, 4>(c, in, out, scale, partial, grid); return;
@@ -807,7 +569,7 @@ void launch_hv_var(Ctx& c, int var, const void* in, void* out, const double* sca
 }
 
 template <typename W, typename R, typename T>
-void launch_hv_nv(Ctx& c, int var, const void* in, void* out, int nv, const double* scale, double* partial,
+void launch_hv_nv(Ctx& c, int var, const void* in, void* out, int nv, const double* scale, fx128* partial,
                   int grid) {
   switch (nv) {
     case 1:
@@ -826,7 +588,7 @@ void launch_hv_nv(Ctx& c, int var, const void* in, void* out, int nv, const doub
 }
 
 void launch_any(Ctx& c, int var, const void* in, void* out, int nv, bool fp32, const double* scale,
-                double* partial, int grid) {
+                fx128* partial, int grid) {
   if (c.wide) {
     if (fp32) launch_hv_nv<uint64_t, uint64_t, float>(c, var, in, out, nv, scale, partial, grid);
     else launch_hv_nv<uint64_t, uint64_t, double>(c, var, in, out, nv, scale, partial, grid);
@@ -839,12 +601,35 @@ void launch_any(Ctx& c, int var, const void* in, void* out, int nv, bool fp32, c
 // Autotuner: the first time an H*V of a given (word size, precision, vectors
 // per sweep, block-size class) runs on a block big enough to measure, every
 // variant is timed on that block (output to the caller's scratch, no state
-// touched) and the fastest is kept for the process. Results do not depend on
-// the variant (same grid, same summation order).
+// touched) and the fastest is kept for the process (FTLM_HV_RETUNE=1: once per
+// context instead). Results do not depend on the variant (same per-row sum
+// order; the dot-product partials are exact fixed-point sums).
 std::mutex g_tune_mu;
-std::map<std::tuple<int, int, int, int, int>, int> g_tuned;
+std::map<uint64_t, int> g_tuned;
 
-int size_class(int64_t dim) {
+}  // namespace
+
+bool hv_tuned_lookup(Ctx& c, uint64_t key, int& var) {
+  auto lt = c.tuned_local.find(key);
+  if (lt != c.tuned_local.end()) {
+    var = lt->second;
+    return true;
+  }
+  if (c.hv_retune) return false;
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  auto it = g_tuned.find(key);
+  if (it == g_tuned.end()) return false;
+  var = it->second;
+  return true;
+}
+
+void hv_tuned_store(Ctx& c, uint64_t key, int var) {
+  c.tuned_local[key] = var;
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  g_tuned[key] = var;
+}
+
+int hv_size_class(int64_t dim) {
   int k = 0;
   while (dim >= 16 && k < 40) {
     dim >>= 2;
@@ -853,9 +638,12 @@ int size_class(int64_t dim) {
   return k;
 }
 
+namespace {
+
 template <typename W>
 int64_t block_csr_device_t(Ctx& c, DBuf& row_ptr, DBuf& col, DBuf& val, DBuf& diag) {
   const int64_t D = c.blk.dim;
+  if (D > 0x7fffffffLL) throw Error(FTLM_ERR_CAPACITY, "block CSR keeps 32-bit columns: block above 2^31 rows");
   CsrParams<W> P;
   P.g = c.geom;
   if constexpr (sizeof(W) == 4) P.v = view32(c);
@@ -917,6 +705,7 @@ template <typename W>
 bool hoplist_build_t(Ctx& c) {
   const int64_t D = c.blk.dim;
   if (D <= 0) return false;
+  if (D > 0xFFFFFFFFLL) return false;  // entries keep 32-bit columns
   CsrParams<W> P;
   P.g = c.geom;
   if constexpr (sizeof(W) == 4) P.v = view32(c);
@@ -999,13 +788,13 @@ int hv_grid(Ctx& c, int nv, bool fp32) {
 
 int hv_variant(Ctx& c, const void* in, void* out, int nv, bool fp32, int grid) {
   if (c.hv_forced >= 0 && c.hv_forced < kNumVariants) return c.hv_forced;
-  const auto key = std::make_tuple((c.wide ? 1 : 0) | (c.hl_active ? 2 : 0), fp32 ? 1 : 0, nv, size_class(c.blk.dim),
-                                   c.device);
-  {
-    std::lock_guard<std::mutex> lock(g_tune_mu);
-    auto it = g_tuned.find(key);
-    if (it != g_tuned.end()) return it->second;
-  }
+  if (c.hl_active && c.hv_rows && nv == (fp32 ? 2 : 1)) return 0;  // k_hv_rows has no variants
+  const uint64_t key = static_cast<uint64_t>((c.wide ? 1 : 0) | (c.hl_active ? 2 : 0)) |
+                       (static_cast<uint64_t>(fp32 ? 1 : 0) << 4) | (static_cast<uint64_t>(nv) << 8) |
+                       (static_cast<uint64_t>(hv_size_class(c.blk.dim)) << 20) |
+                       (static_cast<uint64_t>(c.device) << 32);
+  int known = -1;
+  if (hv_tuned_lookup(c, key, known)) return known;
   if (c.blk.dim < (1 << 15)) return 1;  // too small to measure; launch overhead dominates
   cudaEvent_t e0, e1;
   FTLM_CUDA(cudaEventCreate(&e0));
@@ -1035,12 +824,24 @@ int hv_variant(Ctx& c, const void* in, void* out, int nv, bool fp32, int grid) {
   cudaEventDestroy(e1);
   c.prof.tune_runs += 1;
   c.prof.kernel_launches += 4 * kNumVariants;
-  std::lock_guard<std::mutex> lock(g_tune_mu);
-  g_tuned[key] = best;
+  hv_tuned_store(c, key, best);
   return best;
 }
 
-void hv_apply(Ctx& c, const void* in, void* out, int nv, bool fp32, const double* scale, double* partial,
+int hv_select_source(Ctx& c, int nv, bool fp32) {
+  c.hl_active = false;
+  c.split_active = false;
+  const int64_t D = c.blk.dim;
+  int mode = c.hv_mode;
+  if (mode < 0) mode = D >= (1 << 14) && nv <= (fp32 ? 32 : 16) ? kSrcList : (D >= kSplitMinDim ? kSrcSplit : kSrcFly);
+  if (mode == kSrcList && !hoplist_build(c)) mode = c.hv_mode < 0 && D >= kSplitMinDim ? kSrcSplit : kSrcFly;
+  if (mode == kSrcSplit && !split_prepare(c, nv, fp32)) mode = kSrcFly;
+  c.hl_active = mode == kSrcList;
+  c.split_active = mode == kSrcSplit;
+  return mode;
+}
+
+void hv_apply(Ctx& c, const void* in, void* out, int nv, bool fp32, const double* scale, fx128* partial,
               int grid) {
   if (grid == 0) grid = hv_grid(c, nv, fp32);
   const int var = hv_variant(c, in, out, nv, fp32, grid);

@@ -22,6 +22,8 @@
 #include <thread>
 
 #include "ftlm_internal.h"
+#include "hv_common.cuh"
+#include "ql.cuh"
 
 namespace ftlm {
 
@@ -57,12 +59,15 @@ __global__ void k_state_init(double* st, int NV, int nva) {
   st[S_STEPS * NV + v] = v < nva ? 0.0 : 1.0;
 }
 
-__global__ void k_alpha_fin(int NV, int ncta, const double* __restrict__ partial, double* __restrict__ st,
+// alpha_j = Re<q_j, H q_j>: exact sum of the H*V kernels' fixed-point
+// partials, so it does not depend on their grid or row scheduling.
+__global__ void k_alpha_fin(int NV, int ncta, const fx128* __restrict__ partial, double* __restrict__ st,
                             double* __restrict__ alpha_j) {
   const int v = threadIdx.x;
   if (v >= NV) return;
-  double s = 0.0;
-  for (int b = 0; b < ncta; ++b) s += partial[static_cast<int64_t>(b) * NV + v];
+  fx128 t = 0;
+  for (int b = 0; b < ncta; ++b) t += partial[static_cast<int64_t>(b) * NV + v];
+  const double s = fx_to_double(t);
   alpha_j[v] = s;
   st[S_CA * NV + v] = s * st[S_CUR * NV + v];
   st[S_CB * NV + v] = st[S_BPREV * NV + v] * st[S_PREV * NV + v];
@@ -96,11 +101,18 @@ __global__ void k_beta_fin(int NV, int ncta, const double* __restrict__ partial,
 }
 
 // w_prev <- y - ca*w_cur - cb*w_prev, per-vector |.|^2 partials.
-template <typename T>
+// FLIP (split-spin H*V): y is completed by the flipped-order output,
+// y[q] + f_q y_D[p(q)], and the new vector is also written in the flipped
+// order, x_D[p(q)] = conj(f_q) w[q].
+template <typename T, bool FLIP>
 __global__ void __launch_bounds__(kUpdThreads) k_update(int64_t nchunks, int NV, const typename VT<T>::V* __restrict__ y,
                                                         const typename VT<T>::V* __restrict__ wc,
                                                         typename VT<T>::V* __restrict__ wp,
-                                                        const double* __restrict__ st, double* __restrict__ partial) {
+                                                        const double* __restrict__ st, double* __restrict__ partial,
+                                                        const typename VT<T>::V* __restrict__ yd,
+                                                        typename VT<T>::V* __restrict__ xd,
+                                                        const uint64_t* __restrict__ fmap,
+                                                        const __grid_constant__ FlipPhase ph) {
   using V = typename VT<T>::V;
   constexpr int VPL = VT<T>::VPL;
   const int CPR = NV / VPL;
@@ -117,21 +129,44 @@ __global__ void __launch_bounds__(kUpdThreads) k_update(int64_t nchunks, int NV,
   const int64_t stride = static_cast<int64_t>(gridDim.x) * kUpdThreads;
   for (int64_t i = static_cast<int64_t>(blockIdx.x) * kUpdThreads + tid; i < nchunks; i += stride) {
     const V h = y[i], x = wc[i], p = wp[i];
+    int64_t fi_idx = 0;
+    double fr = 1.0, fim = 0.0;
+    if constexpr (FLIP) {
+      const int64_t row = i / CPR;
+      int64_t pr;
+      flip_coef(__ldg(fmap + row), ph, pr, fr, fim);
+      fi_idx = pr * CPR + (i - row * CPR);
+    }
     V r;
     if constexpr (VPL == 2) {
-      const double r0 = static_cast<double>(h.x) - ca[0] * x.x - cb[0] * p.x;
-      const double r1 = static_cast<double>(h.y) - ca[0] * x.y - cb[0] * p.y;
-      const double r2 = static_cast<double>(h.z) - ca[1] * x.z - cb[1] * p.z;
-      const double r3 = static_cast<double>(h.w) - ca[1] * x.w - cb[1] * p.w;
+      double h0 = h.x, h1 = h.y, h2 = h.z, h3 = h.w;
+      if constexpr (FLIP) {
+        const V d = yd[fi_idx];
+        h0 += fr * d.x - fim * d.y;
+        h1 += fr * d.y + fim * d.x;
+        h2 += fr * d.z - fim * d.w;
+        h3 += fr * d.w + fim * d.z;
+      }
+      const double r0 = h0 - ca[0] * x.x - cb[0] * p.x;
+      const double r1 = h1 - ca[0] * x.y - cb[0] * p.y;
+      const double r2 = h2 - ca[1] * x.z - cb[1] * p.z;
+      const double r3 = h3 - ca[1] * x.w - cb[1] * p.w;
       r = make_float4(static_cast<float>(r0), static_cast<float>(r1), static_cast<float>(r2), static_cast<float>(r3));
       acc[0] += static_cast<double>(r.x) * r.x + static_cast<double>(r.y) * r.y;
       acc[1] += static_cast<double>(r.z) * r.z + static_cast<double>(r.w) * r.w;
     } else {
-      r.x = h.x - ca[0] * x.x - cb[0] * p.x;
-      r.y = h.y - ca[0] * x.y - cb[0] * p.y;
+      double h0 = h.x, h1 = h.y;
+      if constexpr (FLIP) {
+        const V d = yd[fi_idx];
+        h0 += fr * d.x - fim * d.y;
+        h1 += fr * d.y + fim * d.x;
+      }
+      r.x = h0 - ca[0] * x.x - cb[0] * p.x;
+      r.y = h1 - ca[0] * x.y - cb[0] * p.y;
       acc[0] += r.x * r.x + r.y * r.y;
     }
     wp[i] = r;
+    if constexpr (FLIP) xd[fi_idx] = cmul_conj<T>(fr, fim, r);
   }
 #pragma unroll
   for (int e = 0; e < VPL; ++e) red[tid * VPL + e] = acc[e];
@@ -242,64 +277,7 @@ __device__ void tridiag_vector(int r, int t, int nvmax, int ld, int K, const dou
     e[i] = i + 1 < n ? beta[base + static_cast<int64_t>(i) * ld] : 0.0;
     z[i] = i == 0 ? 1.0 : 0.0;
   }
-  const double eps = 2.220446049250313e-16;
-  for (int l = 0; l < n; ++l) {
-    int iter = 0;
-    while (true) {
-      int m = l;
-      for (; m < n - 1; ++m) {
-        const double dd = fabs(d[m]) + fabs(d[m + 1]);
-        if (fabs(e[m]) <= eps * dd) break;
-      }
-      if (m == l) break;
-      if (++iter > 200) {
-        atomicExch(status, 1);
-        break;
-      }
-      double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
-      double rr = hypot(g, 1.0);
-      g = d[m] - d[l] + e[l] / (g + copysign(rr, g));
-      double s = 1.0, c = 1.0, p = 0.0;
-      bool underflow = false;
-      for (int i = m - 1; i >= l; --i) {
-        double f = s * e[i];
-        const double b = c * e[i];
-        rr = hypot(f, g);
-        e[i + 1] = rr;
-        if (rr == 0.0) {
-          d[i + 1] -= p;
-          e[m] = 0.0;
-          underflow = true;
-          break;
-        }
-        s = f / rr;
-        c = g / rr;
-        g = d[i + 1] - p;
-        rr = (d[i] - g) * s + 2.0 * c * b;
-        p = s * rr;
-        d[i + 1] = g + p;
-        g = c * rr - b;
-        f = z[i + 1];
-        z[i + 1] = s * z[i] + c * f;
-        z[i] = c * z[i] - s * f;
-      }
-      if (underflow) continue;
-      d[l] -= p;
-      e[l] = g;
-      e[m] = 0.0;
-    }
-  }
-  for (int i = 1; i < n; ++i) {  // insertion sort, ascending
-    const double dk = d[i], zk = z[i];
-    int j = i - 1;
-    while (j >= 0 && d[j] > dk) {
-      d[j + 1] = d[j];
-      z[j + 1] = z[j];
-      --j;
-    }
-    d[j + 1] = dk;
-    z[j + 1] = zk;
-  }
+  if (!ql_first_row(n, d, z, e)) atomicExch(status, 1);
   double* dr = dout + static_cast<int64_t>(r) * K;
   double* zr = zout + static_cast<int64_t>(r) * K;
   for (int i = 0; i < n; ++i) {
@@ -564,18 +542,17 @@ void run_ftlm_block(Ctx& c, int n_up, int n_dn, int mx, int my, Spectrum& out, c
   int32_t* steps_all = c.ritz_tmp.as<int32_t>();
   std::vector<double> hstart;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> evs;
-  double hv_bytes = 0.0;
+  double hv_bytes = 0.0, hv_hops = 0.0, hv_min_bytes = 0.0;
   // Operator source: the cached hop list pays one lookup pass per block and
-  // then streams 8 B per hop; it pays off when few vectors share each lookup.
-  struct ListGuard {
-    Ctx& c;
-    ~ListGuard() { c.hl_active = false; }
-  } guard{c};
-  bool use_list = c.hv_mode == 1 ||
-                  (c.hv_mode < 0 && D >= (1 << 14) && next_pow2(std::min(nvmax, R)) <= (fp32 ? 32 : 16));
-  if (use_list) use_list = hoplist_build(c);
-  c.hl_active = use_list;
-  const double nzh = c.timing ? static_cast<double>(use_list ? c.hl_nnz : block_nonzero_hops(c)) : 0.0;
+  // then streams 8 B per hop (few vectors share each lookup); large blocks
+  // run the split-spin segment sweeps; the rest the on-the-fly kernel.
+  HvSourceGuard guard{c};
+  const int src = hv_select_source(c, next_pow2(std::max(std::min(nvmax, R), fp32 ? 2 : 1)), fp32);
+  c.prof.hv_source = src;
+  const bool split = src == kSrcSplit;
+  const double nzh = c.timing ? static_cast<double>(src == kSrcList ? c.hl_nnz : block_nonzero_hops(c)) : 0.0;
+  const FlipPhase fph = flip_phase(c);
+  const uint64_t* fmap = split ? c.flip_map.as<uint64_t>() : nullptr;
   for (int s0 = 0; s0 < R; s0 += nvmax) {
     const int nva = std::min(nvmax, R - s0);
     const int NV = next_pow2(std::max(nva, fp32 ? 2 : 1));
@@ -612,10 +589,11 @@ void run_ftlm_block(Ctx& c, int n_up, int n_dn, int mx, int my, Spectrum& out, c
     }
     FTLM_LAUNCH_CHECK();
     FTLM_CUDA(cudaMemsetAsync(c.vec_b.p, 0, bytes, c.stream));
-    const int hgrid = hv_grid(c, NV, fp32);
+    if (split) flip_scatter(c, c.vec_a.p, c.vec_xd.p, NV, fp32);
+    const int hgrid = split ? hv_split_max_grid(c) : hv_grid(c, NV, fp32);
     const int ugrid = std::max(1, std::min<int>(static_cast<int>((nchunks + kUpdThreads - 1) / kUpdThreads),
                                                 c.sm_count * 8));
-    c.partial.ensure(sizeof(double) * static_cast<size_t>(std::max(hgrid, ugrid)) * NV);
+    c.partial.ensure(std::max(sizeof(fx128) * hgrid, sizeof(double) * ugrid) * NV);
     c.lz_state.ensure(sizeof(double) * S_NFIELD * NV);
     double* st = c.lz_state.as<double>();
     double* alpha = c.lz_alpha.as<double>() + static_cast<int64_t>(s0 / nvmax) * K * ld;
@@ -630,18 +608,38 @@ void run_ftlm_block(Ctx& c, int n_up, int n_dn, int mx, int my, Spectrum& out, c
         FTLM_CUDA(cudaEventCreate(&e1));
         FTLM_CUDA(cudaEventRecord(e0, c.stream));
       }
-      hv_apply(c, cur, c.vec_h.p, NV, fp32, st + S_CUR * NV, c.partial.as<double>(), hgrid);
+      int ncta = hgrid;
+      if (split)
+        ncta = hv_apply_split(c, cur, c.vec_xd.p, c.vec_h.p, c.vec_yd.p, NV, fp32, st + S_CUR * NV,
+                              c.partial.as<fx128>());
+      else
+        hv_apply(c, cur, c.vec_h.p, NV, fp32, st + S_CUR * NV, c.partial.as<fx128>(), hgrid);
       if (c.timing) {
         FTLM_CUDA(cudaEventRecord(e1, c.stream));
         evs.emplace_back(e0, e1);
       }
-      k_alpha_fin<<<1, 128, 0, c.stream>>>(NV, hgrid, c.partial.as<double>(), st, alpha + static_cast<int64_t>(j) * ld);
-      if (fp32)
-        k_update<float><<<ugrid, kUpdThreads, 0, c.stream>>>(nchunks, NV, c.vec_h.as<float4>(), static_cast<const float4*>(cur),
-                                                             static_cast<float4*>(prev), st, c.partial.as<double>());
-      else
-        k_update<double><<<ugrid, kUpdThreads, 0, c.stream>>>(nchunks, NV, c.vec_h.as<double2>(), static_cast<const double2*>(cur),
-                                                              static_cast<double2*>(prev), st, c.partial.as<double>());
+      k_alpha_fin<<<1, 128, 0, c.stream>>>(NV, ncta, c.partial.as<fx128>(), st, alpha + static_cast<int64_t>(j) * ld);
+      if (fp32) {
+        using V = float4;
+        if (split)
+          k_update<float, true><<<ugrid, kUpdThreads, 0, c.stream>>>(
+              nchunks, NV, c.vec_h.as<V>(), static_cast<const V*>(cur), static_cast<V*>(prev), st,
+              c.partial.as<double>(), c.vec_yd.as<V>(), c.vec_xd.as<V>(), fmap, fph);
+        else
+          k_update<float, false><<<ugrid, kUpdThreads, 0, c.stream>>>(
+              nchunks, NV, c.vec_h.as<V>(), static_cast<const V*>(cur), static_cast<V*>(prev), st,
+              c.partial.as<double>(), nullptr, nullptr, nullptr, fph);
+      } else {
+        using V = double2;
+        if (split)
+          k_update<double, true><<<ugrid, kUpdThreads, 0, c.stream>>>(
+              nchunks, NV, c.vec_h.as<V>(), static_cast<const V*>(cur), static_cast<V*>(prev), st,
+              c.partial.as<double>(), c.vec_yd.as<V>(), c.vec_xd.as<V>(), fmap, fph);
+        else
+          k_update<double, false><<<ugrid, kUpdThreads, 0, c.stream>>>(
+              nchunks, NV, c.vec_h.as<V>(), static_cast<const V*>(cur), static_cast<V*>(prev), st,
+              c.partial.as<double>(), nullptr, nullptr, nullptr, fph);
+      }
       k_beta_fin<<<1, 128, 0, c.stream>>>(NV, ugrid, c.partial.as<double>(), st, beta + static_cast<int64_t>(j) * ld, j, K);
       FTLM_LAUNCH_CHECK();
       c.prof.kernel_launches += 3;
@@ -655,6 +653,8 @@ void run_ftlm_block(Ctx& c, int n_up, int n_dn, int mx, int my, Spectrum& out, c
       // h_nz*D = nonzero-amplitude hops to active targets, m = 8 B per row
       const double s = fp32 ? 8.0 : 16.0;
       hv_bytes += (static_cast<double>(D) * nva * s * 2.0 + nzh * nva * s + static_cast<double>(D) * 8.0) * K;
+      hv_hops += nzh * nva * K;
+      hv_min_bytes += static_cast<double>(D) * (2.0 * nva * s + 8.0) * K;
     }
     c.last_kdim = K;
     c.last_nv = NV;
@@ -687,6 +687,8 @@ void run_ftlm_block(Ctx& c, int n_up, int n_dn, int mx, int my, Spectrum& out, c
       cudaEventDestroy(pr.second);
     }
     c.prof.hv_bytes += hv_bytes;
+    c.prof.hv_hops += hv_hops;
+    c.prof.hv_min_bytes += hv_min_bytes;
   }
   out.prefactor = static_cast<double>(D);
   out.particles = n_up + n_dn;

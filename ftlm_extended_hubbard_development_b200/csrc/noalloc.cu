@@ -10,12 +10,15 @@
 // file-scope device array below, of a fixed size, which every GPU that loads
 // the library holds until the process exits. The first call on a device
 // looks up that array's device address (cudaGetSymbolAddress); make that
-// first call before any stream capture.
+// first call before any stream capture. The address is kept per device and
+// CUDA context, so a call after a device reset looks it up again (that call
+// is then a first call again).
 //
 // The computation is the same as the engine's own Ritz stage: implicit QL
 // with shifts on each tridiagonal, tracking the first row of the eigenvector
 // matrix, an ascending sort, weights v1^2 * inv_samples, spectra concatenated
 // sample by sample.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -23,6 +26,7 @@
 #include <mutex>
 
 #include "../../include/ftlm_gpu.h"
+#include "ql.cuh"
 
 namespace {
 
@@ -35,9 +39,29 @@ constexpr int kMaxNvec = 128;
 __device__ __align__(256) double g_noalloc_scratch[3 * FTLM_NOALLOC_MAX_ENTRIES + 32];
 
 // Device address of g_noalloc_scratch per device ordinal, set up on the first
-// call on that device (host code cannot use the symbol itself as an address).
+// call on that device (host code cannot use the symbol itself as an address),
+// together with the CUDA context it belongs to: after a device reset the
+// runtime creates a new context with the module loaded again, and the
+// address is looked up again there.
 std::mutex g_mu;
 double* g_scratch_addr[64] = {nullptr};
+CUcontext g_scratch_ctx[64] = {nullptr};
+
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+
+// cuCtxGetCurrent through the runtime's driver entry-point table (no link
+// against the driver library); null when it cannot be resolved.
+CtxGetCurrentFn ctx_get_current() {
+  static const CtxGetCurrentFn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return static_cast<CtxGetCurrentFn>(nullptr);
+    return reinterpret_cast<CtxGetCurrentFn>(p);
+  }();
+  return fn;
+}
 
 void set_err(char* buf, size_t len, const char* msg) {
   if (buf && len) {
@@ -66,62 +90,7 @@ __global__ void k_ritz_noalloc(const double* __restrict__ alpha, const double* _
       e[i] = i + 1 < n ? beta[static_cast<int64_t>(v) * ld + i] : 0.0;
       z[i] = i == 0 ? 1.0 : 0.0;
     }
-    const double eps = 2.220446049250313e-16;
-    for (int l = 0; l < n; ++l) {
-      int iter = 0;
-      while (true) {
-        int m = l;
-        for (; m < n - 1; ++m)
-          if (fabs(e[m]) <= eps * (fabs(d[m]) + fabs(d[m + 1]))) break;
-        if (m == l) break;
-        if (++iter > 200) {
-          atomicExch(&failed, 1);
-          break;
-        }
-        double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
-        double r = hypot(g, 1.0);
-        g = d[m] - d[l] + e[l] / (g + copysign(r, g));
-        double s = 1.0, c = 1.0, p = 0.0;
-        bool underflow = false;
-        for (int i = m - 1; i >= l; --i) {
-          double f = s * e[i];
-          const double b = c * e[i];
-          r = hypot(f, g);
-          e[i + 1] = r;
-          if (r == 0.0) {
-            d[i + 1] -= p;
-            e[m] = 0.0;
-            underflow = true;
-            break;
-          }
-          s = f / r;
-          c = g / r;
-          g = d[i + 1] - p;
-          r = (d[i] - g) * s + 2.0 * c * b;
-          p = s * r;
-          d[i + 1] = g + p;
-          g = c * r - b;
-          f = z[i + 1];
-          z[i + 1] = s * z[i] + c * f;
-          z[i] = c * z[i] - s * f;
-        }
-        if (underflow) continue;
-        d[l] -= p;
-        e[l] = g;
-        e[m] = 0.0;
-      }
-    }
-    for (int i = 1; i < n; ++i) {
-      const double dk = d[i], zk = z[i];
-      int j = i - 1;
-      while (j >= 0 && d[j] > dk) {
-        d[j + 1] = d[j];
-        z[j + 1] = z[j];
-        --j;
-      }
-      d[j + 1] = dk;
-      z[j + 1] = zk;
-    }
+    if (!ftlm::ql_first_row(n, d, z, e)) atomicExch(&failed, 1);
   }
   __syncthreads();
   if (v == 0) {
@@ -176,6 +145,11 @@ extern "C" int ftlm_ritz_noalloc(const double* alpha, const double* beta, const 
   double* scratch = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_mu);
+    CUcontext cur = nullptr;
+    const CtxGetCurrentFn get = ctx_get_current();
+    if (get) get(&cur);
+    if (!get || cur != g_scratch_ctx[dev]) g_scratch_addr[dev] = nullptr;  // new context: look it up again
+    g_scratch_ctx[dev] = cur;
     if (!g_scratch_addr[dev]) {
       // first call on this device: resolve the array's device address
       void* p = nullptr;

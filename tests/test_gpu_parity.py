@@ -43,6 +43,15 @@ def sectors_by_case(golden):
     return out
 
 
+def test_loaded_device_code_is_sm100():
+    """The runtime loaded this library's sm_100a SASS (no PTX JIT path)."""
+    import ctypes as C
+    lib = pkg.load_library()
+    bv, pv = C.c_int32(0), C.c_int32(-1)
+    assert lib.ftlm_device_code_version(0, C.byref(bv), C.byref(pv)) == 0
+    assert bv.value == 100 and pv.value == 0, (bv.value, pv.value)
+
+
 def test_sector_basis_relations_and_csr_bit_exact(golden, sectors_by_case):
     checked_blocks = 0
     for case, secs in sectors_by_case.items():
