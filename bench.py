@@ -108,20 +108,18 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def ncu_traffic(args):
-    """DRAM bytes per H*V launch of the bench block, from the committed
-    one-pass ncu summary (profiles/k_hv_4x4_sector88_nv128_mixed_traffic.md);
-    None for any other workload than the default one it was captured on."""
+def ncu_traffic(args, split):
+    """DRAM bytes per H*V application of the bench block, from the committed
+    ncu captures (profiles/traffic.json; each entry names its capture and how
+    it scales to the bench block); None for any other workload."""
     if SECTOR != (8, 8) or STEPS <= 0 or args.precision != "mixed" or args.batch not in (0, 128):
         return None
-    p = os.path.join(HERE, "profiles", "k_hv_4x4_sector88_nv128_mixed_traffic.md")
+    key = "split_4x4_sector88_nv128_mixed" if split else "fly_4x4_sector88_nv128_mixed"
     try:
-        for line in open(p):
-            if line.startswith("dram_bytes_per_launch:"):
-                return float(line.split(":")[1])
-    except OSError:
-        pass
-    return None
+        with open(os.path.join(HERE, "profiles", "traffic.json")) as f:
+            return float(json.load(f)[key]["dram_bytes_per_launch"])
+    except (OSError, KeyError, ValueError):
+        return None
 
 
 def cpu_baseline(threads: int, sweeps: int = 2, skip: int = 0):
@@ -144,6 +142,8 @@ def cpu_baseline(threads: int, sweeps: int = 2, skip: int = 0):
     gbs = bytes_per_sweep * len(per) / sum(per) / 1e9
     return {"value": gbs, "unit": "GB/s", "cores": j["threads"], "kind": "reference",
             "per_sweep_gbs": [bytes_per_sweep / s / 1e9 for s in per],
+            "dim": D, "vectors": nv, "nonzero_hops": nz,
+            "hop_vector_products_per_s": nz * nv * len(per) / sum(per),
             "sample": (f"reference apply_hamiltonian (FP64 CSR SpMV, OpenMP over vectors) on 4x4 U=7 "
                        f"sector (4,4) k=(0,0), dim {D}, {nv} vectors x {len(per)} timed sweeps "
                        f"({sum(per):.3f} s); sector (8,8) itself needs ~15 min and ~30 GB to build on the CPU")}
@@ -163,7 +163,16 @@ def run_reference(args):
             "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "c128", "data": "synthetic (model-defined Hilbert space, Gaussian vectors)",
             "impl": "reference",
-            "config": {"workload": "4x4 U=7 t'=0 FTLM H*V, sector (8,8) k=(0,0), 128 vectors x 80 steps"},
+            "config": {"workload": (f"4x4 U=7 t'=0 H*V of the reference's apply_hamiltonian (FP64 CSR SpMV, "
+                                    f"OpenMP over vectors, {base['cores']} host threads) on sector (4,4) "
+                                    f"k=(0,0), dim {base['dim']}, {base['vectors']} vectors per sweep: the "
+                                    f"largest 4x4 U=7 block the reference builds within a bench step "
+                                    f"(the GPU arm's sector (8,8) block needs ~15 min and ~30 GB to build "
+                                    f"on the CPU)"),
+                       "lattice": "4x4", "sector": [4, 4], "k": [0, 0], "dim": base["dim"],
+                       "vectors_per_sweep": base["vectors"], "precision": "fp64", "threads": base["cores"]},
+            "rate": {"hop_vector_products_per_s": base["hop_vector_products_per_s"],
+                     "note": "nonzero off-diagonal hops x vectors per second: precision-neutral"},
             "cpu_baseline": {**base, "value": v},
             "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -217,9 +226,20 @@ def run_ours(args):
         torch.distributed.all_reduce(b, op=torch.distributed.ReduceOp.SUM)
     dev_s_max, bytes_all = float(t.item()), float(b.item())
     value = bytes_all / dev_s_max / 1e9
-    achieved = prof["hv_bytes"] / (prof["hv_ms"] / 1e3) / 1e9
+    split = prof["hv_source"] == 2
     peak, peak_kind = hbm_peak()
-    bytes_per_launch = prof["hv_bytes"] / max(prof["hv_launches"], 1)
+    launches = max(prof["hv_launches"], 1)
+    hv_s = prof["hv_ms"] / 1e3
+    # Roofline bytes of the dominant kernel. The on-the-fly kernel gathers every
+    # hop's row from HBM: the gather model D*[nv*s*(1+h_nz) + nv*s + 8]. The
+    # split-spin sweeps gather only inside the L2-resident segment of the row
+    # being processed, so their HBM bytes are the compulsory D*(2*nv*s + 8) per
+    # sweep, two sweeps (both row orders) per H*V; the gather model over their
+    # time is reported beside it as the L2-served rate.
+    model_bytes = prof["hv_bytes"] / launches
+    roof_bytes = (2.0 * prof["hv_min_bytes"] if split else prof["hv_bytes"]) / launches
+    achieved = roof_bytes / (hv_s / launches) / 1e9
+    bytes_per_launch = roof_bytes
 
     # e2e through the C ABI: tables from the model, spectrum and thermodynamic
     # sums read back to host buffers every step
@@ -260,11 +280,19 @@ def run_ours(args):
                        "parallelism": f"weak: one k-block per rank x{ws}"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
-                         "kernel": ("k_hv_list (cached hop list)" if 0 < args.batch <= 32
-                                    else "k_hv (on-the-fly multi-vector H*V)"),
+                         "kernel": (["k_hv (on-the-fly multi-vector H*V)", "k_hv_list (cached hop list)",
+                                     "k_hv_seg x2 (split-spin segment sweeps, both row orders)"]
+                                    [prof["hv_source"]] if prof["hv_source"] in (0, 1, 2) else "unknown"),
                          "kernel_variant": prof["hv_variant"],
                          "bytes_per_launch": bytes_per_launch,
-                         "traffic": ncu_traffic(args)},
+                         "bytes_model": ("compulsory: 2 sweeps x D*(2*nv*s + 8)" if split else
+                                         "gather model: D*[nv*s*(1+h_nz) + nv*s + 8]"),
+                         "gather_model_bytes_per_launch": model_bytes,
+                         "gather_model_gbs": model_bytes / (hv_s / launches) / 1e9,
+                         "traffic": ncu_traffic(args, split)},
+            "rate": {"hop_vector_products_per_s": prof["hv_hops"] / dev_s,
+                     "hv_kernel_hop_vector_products_per_s": prof["hv_hops"] / hv_s,
+                     "note": "nonzero off-diagonal hops x vectors per second: precision-neutral"},
             "e2e": {"value": e2e_val, "unit": "GB/s",
                     "h2d_bytes_per_step": pe["h2d_bytes"] / args.steps,
                     "d2h_bytes_per_step": pe["d2h_bytes"] / args.steps},
