@@ -16,7 +16,11 @@ nonzero-amplitude hops per row, m = 8 B per row). `value` divides by the
 whole step (Lanczos updates, reductions, tridiagonal solve included);
 `roofline.achieved` divides by the H*V kernel's own CUDA-event time.
 
-  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+With --workload 6x3 the block is the large bandwidth-bound one instead: 6x3
+torus (18 sites), t'=0.2, U=8, V=1.5, twist (0.25, 0.5), sector
+N_up=N_down=9, k=(0,0), dim ~1.31e8, 16 vectors x 100 steps, mixed precision.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--workload 4x4|6x3]
 """
 from __future__ import annotations
 
@@ -33,9 +37,24 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 
 METRIC = "H*v HBM GB/s; sec per n(mu) curve, mixed vs FP64 GPU at |dn|<=1e-4"
-MODEL = dict(lx=4, ly=4, tx=1.0, ty=1.0, tp=0.0, phix=1.0, phiy=1.0, u=7.0, v=0.0)
-SECTOR = (8, 8)
-SAMPLES, STEPS = 128, 80
+# Block workloads (one bench step = the FTLM of one momentum block):
+#  4x4: the largest block of the batched 4x4 production curve (the metric's
+#       workload); 6x3: the large bandwidth-bound block, 6x3 half filling.
+# `ref` is the bounded CPU sample of the reference's own apply_hamiltonian:
+# the same couplings on the largest sector of the lattice that the reference
+# builds within seconds.
+WORKLOADS = {
+    "4x4": dict(model=dict(lx=4, ly=4, tx=1.0, ty=1.0, tp=0.0, phix=1.0, phiy=1.0, u=7.0, v=0.0),
+                sector=(8, 8), samples=128, steps=80, betas=[2.857142857142857, 12.5], mu=(-3.0, 4.0, 281),
+                name="4x4 U=7 t'=0", ref_sector=(4, 4)),
+    "6x3": dict(model=dict(lx=6, ly=3, tx=1.0, ty=1.0, tp=0.2, phix=0.25, phiy=0.5, u=8.0, v=1.5),
+                sector=(9, 9), samples=16, steps=100, betas=[10.0], mu=(-4.0, 8.0, 121),
+                name="6x3 U=8 V=1.5 t'=0.2 twist (0.25,0.5)", ref_sector=(3, 4)),
+}
+WL = "4x4"
+MODEL = WORKLOADS[WL]["model"]
+SECTOR = WORKLOADS[WL]["sector"]
+SAMPLES, STEPS = WORKLOADS[WL]["samples"], WORKLOADS[WL]["steps"]
 FALLBACK_HBM = 6650.0
 
 
@@ -112,9 +131,9 @@ def ncu_traffic(args, split):
     """DRAM bytes per H*V application of the bench block, from the committed
     ncu captures (profiles/traffic.json; each entry names its capture and how
     it scales to the bench block); None for any other workload."""
-    if SECTOR != (8, 8) or STEPS <= 0 or args.precision != "mixed" or args.batch not in (0, 128):
+    if SECTOR != WORKLOADS[WL]["sector"] or STEPS <= 0 or args.precision != "mixed" or args.batch != 0:
         return None
-    key = "split_4x4_sector88_nv128_mixed" if split else "fly_4x4_sector88_nv128_mixed"
+    key = ("split_" if split else "fly_") + {"4x4": "4x4_sector88_nv128_mixed", "6x3": "6x3_sector99_nv16_mixed"}[WL]
     try:
         with open(os.path.join(HERE, "profiles", "traffic.json")) as f:
             return float(json.load(f)[key]["dram_bytes_per_launch"])
@@ -125,13 +144,20 @@ def ncu_traffic(args, split):
 def cpu_baseline(threads: int, sweeps: int = 2, skip: int = 0):
     """The reference's own apply_hamiltonian (oracle/_ref/ref_bench, compiled
     from the reference sources) on a bounded sample: same lattice and
-    couplings, the largest sector it builds in seconds (4x4 (4,4), ~15 s),
-    16 vectors per sweep; the first `skip` sweeps are warm-up."""
+    couplings, the largest sector it builds in seconds (4x4: (4,4), ~15 s;
+    6x3: (3,4), ~15 s), 16 vectors per sweep; the first `skip` sweeps are
+    warm-up."""
     exe = os.path.join(HERE, "oracle", "_ref", "ref_bench")
     if not os.path.exists(exe):
         return None
-    args = [exe, "hv", "4", "4", "0", "0", "16", str(sweeps + skip), "--", "--lx", "4", "--ly", "4",
-            "--u", "7", "--threads", str(threads), "--max-sector-dim", "100000000"]
+    w = WORKLOADS[WL]
+    m = w["model"]
+    nu, nd = w["ref_sector"]
+    flags = []
+    for k in ("lx", "ly", "tx", "ty", "tp", "phix", "phiy", "u", "v"):
+        flags += ["--" + k, repr(m[k]) if isinstance(m[k], float) else str(m[k])]
+    args = [exe, "hv", str(nu), str(nd), "0", "0", "16", str(sweeps + skip), "--"] + flags + [
+        "--threads", str(threads), "--max-sector-dim", "100000000"]
     r = subprocess.run(args, capture_output=True, text=True, env={**os.environ, "OPENBLAS_NUM_THREADS": "1"})
     if r.returncode != 0:
         return None
@@ -144,9 +170,11 @@ def cpu_baseline(threads: int, sweeps: int = 2, skip: int = 0):
             "per_sweep_gbs": [bytes_per_sweep / s / 1e9 for s in per],
             "dim": D, "vectors": nv, "nonzero_hops": nz,
             "hop_vector_products_per_s": nz * nv * len(per) / sum(per),
-            "sample": (f"reference apply_hamiltonian (FP64 CSR SpMV, OpenMP over vectors) on 4x4 U=7 "
-                       f"sector (4,4) k=(0,0), dim {D}, {nv} vectors x {len(per)} timed sweeps "
-                       f"({sum(per):.3f} s); sector (8,8) itself needs ~15 min and ~30 GB to build on the CPU")}
+            "sample": (f"reference apply_hamiltonian (FP64 CSR SpMV, OpenMP over vectors) on {w['name']} "
+                       f"sector ({nu},{nd}) k=(0,0), dim {D}, {nv} vectors x {len(per)} timed sweeps "
+                       f"({sum(per):.3f} s); the GPU block's sector {w['sector']} is beyond the reference "
+                       f"on this host (4x4 (8,8): ~15 min and ~30 GB to build; 6x3 (9,9): its 32-bit "
+                       f"CSR overflows and it needs ~300 GB)")}
 
 
 def run_reference(args):
@@ -163,13 +191,13 @@ def run_reference(args):
             "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "c128", "data": "synthetic (model-defined Hilbert space, Gaussian vectors)",
             "impl": "reference",
-            "config": {"workload": (f"4x4 U=7 t'=0 H*V of the reference's apply_hamiltonian (FP64 CSR SpMV, "
-                                    f"OpenMP over vectors, {base['cores']} host threads) on sector (4,4) "
-                                    f"k=(0,0), dim {base['dim']}, {base['vectors']} vectors per sweep: the "
-                                    f"largest 4x4 U=7 block the reference builds within a bench step "
-                                    f"(the GPU arm's sector (8,8) block needs ~15 min and ~30 GB to build "
-                                    f"on the CPU)"),
-                       "lattice": "4x4", "sector": [4, 4], "k": [0, 0], "dim": base["dim"],
+            "config": {"workload": (f"{WORKLOADS[WL]['name']} H*V of the reference's apply_hamiltonian "
+                                    f"(FP64 CSR SpMV, OpenMP over vectors, {base['cores']} host threads) on "
+                                    f"sector {WORKLOADS[WL]['ref_sector']} k=(0,0), dim {base['dim']}, "
+                                    f"{base['vectors']} vectors per sweep: the largest block of this lattice "
+                                    f"the reference builds within a bench step (the GPU arm's sector "
+                                    f"{WORKLOADS[WL]['sector']} is beyond it on this host)"),
+                       "lattice": WL, "sector": list(WORKLOADS[WL]["ref_sector"]), "k": [0, 0], "dim": base["dim"],
                        "vectors_per_sweep": base["vectors"], "precision": "fp64", "threads": base["cores"]},
             "rate": {"hop_vector_products_per_s": base["hop_vector_products_per_s"],
                      "note": "nonzero off-diagonal hops x vectors per second: precision-neutral"},
@@ -243,8 +271,8 @@ def run_ours(args):
 
     # e2e through the C ABI: tables from the model, spectrum and thermodynamic
     # sums read back to host buffers every step
-    mu = pkg.linspace(-3.0, 4.0, 281)
-    betas = np.array([2.857142857142857, 12.5])
+    mu = pkg.linspace(*WORKLOADS[WL]["mu"])
+    betas = np.array(WORKLOADS[WL]["betas"])
     eng.profile_reset()
     barrier()
     t0 = time.perf_counter()
@@ -270,13 +298,13 @@ def run_ours(args):
             "scaling": "weak", "vs_baseline": None,
             "dtype": "c64 vectors, f64 reductions" if prec == pkg.engine.PREC_MIXED else "c128",
             "data": "synthetic (model-defined Hilbert space; Philox uniform-phase start vectors)",
-            "config": {"workload": (f"4x4 U=7 t'=0 FTLM block, sector (8,8) k=({mx},{my}) dim {dim}: "
-                                    f"{SAMPLES} vectors x {STEPS} Lanczos steps per step, "
+            "config": {"workload": (f"{WORKLOADS[WL]['name']} FTLM block, sector {SECTOR} k=({mx},{my}) "
+                                    f"dim {dim}: {SAMPLES} vectors x {STEPS} Lanczos steps per step, "
                                     f"{args.precision}"),
-                       "lattice": "4x4", "sector": list(SECTOR), "k": [mx, my], "dim": dim,
+                       "lattice": WL, "model": MODEL, "sector": list(SECTOR), "k": [mx, my], "dim": dim,
                        "samples": SAMPLES, "lanczos_steps": STEPS, "precision": args.precision,
                        "batch_vectors": args.batch or min(SAMPLES, 128),
-                       "l2": "inputs larger than L2 (3 vector arrays of dim x 128 x 8 B each)",
+                       "l2": "inputs larger than L2 (vector arrays of dim x vectors x 8 B each)",
                        "parallelism": f"weak: one k-block per rank x{ws}"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
@@ -444,7 +472,7 @@ def run_curve_mode(args):
 
 
 def main():
-    global SECTOR, STEPS
+    global SECTOR, STEPS, WL, MODEL, SAMPLES
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
@@ -453,8 +481,10 @@ def main():
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--batch", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--sector", default="8,8", help="N_up,N_down of the 4x4 sector (profiling cases)")
-    ap.add_argument("--lanczos-steps", type=int, default=STEPS)
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="4x4",
+                    help="4x4: 4x4 U=7 (8,8) block, 128 x 80 (default); 6x3: 6x3 (9,9) block, 16 x 100")
+    ap.add_argument("--sector", default="", help="N_up,N_down of another sector of the lattice (profiling cases)")
+    ap.add_argument("--lanczos-steps", type=int, default=0)
     ap.add_argument("--curve", choices=sorted(CURVES), help="time whole n(mu) curves instead")
     ap.add_argument("--plain-sectors", default="", help="'nu,nd;nu,nd': run the FP64 plain path on these only")
     ap.add_argument("--plain-samples", type=int, default=0)
@@ -465,8 +495,11 @@ def main():
         else:
             run_curve_mode(args)
         return
-    SECTOR = tuple(int(x) for x in args.sector.split(","))
-    STEPS = args.lanczos_steps
+    WL = args.workload
+    w = WORKLOADS[WL]
+    MODEL, SAMPLES = w["model"], w["samples"]
+    SECTOR = tuple(int(x) for x in args.sector.split(",")) if args.sector else w["sector"]
+    STEPS = args.lanczos_steps or w["steps"]
     if args.impl == "reference":
         run_reference(args)
     else:
