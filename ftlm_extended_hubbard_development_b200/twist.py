@@ -122,9 +122,20 @@ def curve_at_twist(model: Model, phix: float, phiy: float, betas, mu, opts: RunO
     return run_curve(replace(model, phix=float(phix), phiy=float(phiy)), betas, mu, opts, ed=ed)
 
 
-def run_twist_grid(model: Model, twists, betas, mu, opts: RunOpts | None = None, ed: bool = False):
-    """Engine n(mu) curves at each twist: list of (phix, phiy, curve)."""
-    return [(px, py, curve_at_twist(model, px, py, betas, mu, opts, ed)) for px, py in twists]
+def twist_owners(n_twists: int, world: int):
+    """Rank of each twist: the curves at different twists cost the same, so
+    longest-processing-time assignment is a deal in list order."""
+    return [i % world for i in range(n_twists)]
+
+
+def run_twist_grid(model: Model, twists, betas, mu, opts: RunOpts | None = None, ed: bool = False,
+                   rank: int = 0, world: int = 1):
+    """Engine n(mu) curves at this rank's twists (all of them with one rank):
+    list of (phix, phiy, curve). Ranks share nothing while running; gather
+    the lists (e.g. torch.distributed.all_gather_object) to combine them."""
+    own = twist_owners(len(twists), world)
+    return [(px, py, curve_at_twist(model, px, py, betas, mu, opts, ed))
+            for i, (px, py) in enumerate(twists) if own[i] == rank]
 
 
 def uniform_grid(n: int):

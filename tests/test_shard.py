@@ -40,16 +40,48 @@ def _accumulate(blocks):
     return emin, z, n, n2
 
 
-def test_sector_owners_cover_and_balance():
-    for sites, world in ((8, 2), (16, 8), (18, 3), (4, 5)):
-        own = shard.sector_owners(sites, world)
-        assert sorted(own) == [(a, b) for a in range(sites + 1) for b in range(sites + 1)]
-        load = [0] * world
-        for (a, b), r in own.items():
-            load[r] += comb(sites, a) * comb(sites, b)
-        biggest = comb(sites, sites // 2) ** 2
-        assert max(load) - min(load) <= biggest
-    assert shard.sector_owners(8, 1) == {s: 0 for s in shard.sector_owners(8, 1)}
+def test_block_dims_host_match_reference_goldens(golden):
+    """Character counting on the host gives the reference's block
+    dimensions (main.cpp:745-766) for every sector of the golden lattices."""
+    n = 0
+    for case, nu, nd in golden.sector_keys():
+        c = golden.cases[case]
+        want = golden.sec(case, nu, nd, "block_dim")
+        assert shard.block_dims_host(c["lx"], c["ly"], nu, nd) == list(want), (case, nu, nd)
+        n += 1
+    assert n > 100
+
+
+def test_block_owners_cover_and_balance():
+    for lx, ly, world in ((4, 2, 2), (3, 3, 3), (4, 4, 8), (2, 2, 5)):
+        m = shard.Model(lx=lx, ly=ly, tp=0.2)
+        opts = shard.RunOpts(samples=32, lanczos_steps=80, exact_block_threshold=256)
+        own = shard.block_owners(m, world, opts)
+        want = {(a, b, k % lx, k // lx) for a in range(m.sites + 1) for b in range(m.sites + 1)
+                for k, d in enumerate(shard.block_dims_host(lx, ly, a, b)) if d > 0}
+        assert set(own) == want and set(own.values()) <= set(range(world))
+        load = [0.0] * world
+        big = 0.0
+        for (a, b, mx, my), r in own.items():
+            d = shard.block_dims_host(lx, ly, a, b)[my * lx + mx]
+            h = sum((4 + 4) * p * (m.sites - p) / max(m.sites - 1, 1) for p in (a, b))
+            c = shard.block_cost(d, d <= 256, 32, 80, h)
+            load[r] += c
+            big = max(big, c)
+        assert max(load) - min(load) <= big  # LPT bound
+    m = shard.Model(lx=4, ly=2)
+    assert set(shard.block_owners(m, 1).values()) == {0}
+
+
+def test_config5_sector_splits_over_two_ranks():
+    """The 6x3 (9,9) sector is 18 k-blocks of ~1.313e8 rows: two ranks take
+    9 each (one sector no longer lands on one rank)."""
+    m = shard.Model(lx=6, ly=3, tp=0.2, phix=0.25, phiy=0.5, u=8.0, v=1.5)
+    opts = shard.RunOpts(samples=16, lanczos_steps=100)
+    own = shard.block_owners(m, 2, opts, sectors=[(9, 9)])
+    assert len(own) == 18
+    per = [sum(1 for r in own.values() if r == k) for k in range(2)]
+    assert per == [9, 9]
 
 
 def _worker(rank, world, port, q):
@@ -70,6 +102,40 @@ def _free_port():
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
         return s.getsockname()[1]
+
+
+def _plan_worker(rank, world, port, q):
+    import torch
+    import torch.distributed as dist
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
+    try:
+        m = shard.Model(lx=6, ly=3, tp=0.2, phix=0.25, phiy=0.5, u=8.0, v=1.5)
+        own = shard.block_owners(m, world, shard.RunOpts(samples=16, lanczos_steps=100), sectors=[(9, 9)])
+        mine = sorted(k for k, r in own.items() if r == rank)
+        t = torch.zeros(18, dtype=torch.int64)
+        for (_, _, mx, my) in mine:
+            t[my * 6 + mx] = rank + 1
+        dist.all_reduce(t)  # every block claimed by exactly one rank
+        q.put((rank, t.tolist(), len(mine)))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_config5_plan_agrees_across_gloo_ranks():
+    world = 2
+    ctx = tmp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_plan_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    got = dict((r, (t, n)) for r, t, n in (q.get(timeout=120) for _ in range(world)))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for r in range(world):
+        t, n = got[r]
+        assert n == 9 and sorted(t) == [1] * 9 + [2] * 9
 
 
 def test_merge_over_gloo_equals_single_accumulation():
