@@ -112,6 +112,32 @@ CLI_RUNS = {
 }
 
 
+# Per-block trace and selected-block debug outputs (main.cpp:1583-1663,
+# 1233-1267): name -> (args, selected block (nup, ndown, mx, my)).
+TRACE_RUNS = {
+    "config1_t0": (CONFIG1 + ["--exact-block-threshold", "0"], (2, 2, 0, 0)),
+    # 3x2 with t', V and twists; the reference's trace mode ends in SIGSEGV on
+    # 4x2 lattices in this build (its ftlm_n_vs_mu with OpenMP + OpenBLAS
+    # 0.3.15), while 2x2 and 3x2 run to completion.
+    "c3x2_t0": (CLI_RUNS["c3x2_t0"][1], (3, 2, 1, 1)),
+}
+
+
+def write_trace_goldens(csvdir, tmp):
+    """Reference trace and debug CSVs of TRACE_RUNS into csv/<name>_trace.csv
+    and csv/<name>_debug.csv (plus the run's stdout)."""
+    for name, (cli, (nu, nd, mx, my)) in TRACE_RUNS.items():
+        tr = os.path.join(csvdir, name + "_trace.csv")
+        dbg = os.path.join(csvdir, name + "_debug.csv")
+        r = run([os.path.join(REF, "ftlm_n_vs_mu")] + cli + [
+            "--output", os.path.join(tmp, name + ".csv"), "--trace-partition-csv", tr,
+            "--debug-block-nup", str(nu), "--debug-block-ndown", str(nd), "--debug-block-mx", str(mx),
+            "--debug-block-my", str(my), "--debug-block-csv", dbg])
+        with open(os.path.join(csvdir, name + "_trace.stdout"), "w") as f:
+            f.write(r.stdout)
+    return {k: {"exe": "ftlm_n_vs_mu", "args": v[0], "block": list(v[1])} for k, v in TRACE_RUNS.items()}
+
+
 def run(cmd, **kw):
     r = subprocess.run(cmd, capture_output=True, text=True, **kw)
     if r.returncode != 0:
@@ -134,11 +160,24 @@ def load_dir(d):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--skip-slow", action="store_true")
+    ap.add_argument("--only-trace", action="store_true",
+                    help="write only the trace/debug fixtures and their cases.json entry")
     args = ap.parse_args()
     for b in ("ref_probe", "ftlm_n_vs_mu", "ftlm_ed_n_vs_mu"):
         if not os.path.exists(os.path.join(REF, b)):
             raise SystemExit("reference binaries missing: run `make -C oracle ref` first")
     tmp = tempfile.mkdtemp()
+    if args.only_trace:
+        try:
+            path = os.path.join(HERE, "cases.json")
+            with open(path) as f:
+                meta = json.load(f)
+            meta["trace_runs"] = write_trace_goldens(os.path.join(HERE, "csv"), tmp)
+            with open(path, "w") as f:
+                json.dump(meta, f, indent=1)
+        finally:
+            shutil.rmtree(tmp, ignore_errors=True)
+        return
     try:
         sectors = {}
         for case, which in SECTOR_DUMPS:
@@ -189,8 +228,10 @@ def main():
             "--checkpoint", ck, "--output", os.path.join(tmp, "ck.csv")])
         shutil.copy(os.path.join(tmp, "ck.csv"), os.path.join(csvdir, "config1_ckpt.csv"))
 
+        trace_runs = write_trace_goldens(csvdir, tmp)
         meta = {"cases": CASES,
                 "cli_runs": {k: {"exe": v[0], "args": v[1]} for k, v in CLI_RUNS.items()},
+                "trace_runs": trace_runs,
                 "checkpoint_run": {"exe": "ftlm_n_vs_mu",
                                    "args": CONFIG1 + ["--exact-block-threshold", "4"]},
                 "lanczos_dumps": LANCZOS_DUMPS, "exact_dumps": EXACT_DUMPS,
