@@ -355,9 +355,11 @@ PATHS = {
 }
 
 
-def time_curve(pkg, cfg, path, sectors=None, samples=None):
+def time_curve(pkg, cfg, path, sectors=None, samples=None, per_sector=None):
     """Wall time of one n(mu) curve through the C ABI (block order of the
-    reference), or of the listed sectors only; returns (seconds, observables)."""
+    reference), or of the listed sectors only; returns (seconds, observables).
+    per_sector (a dict) receives each sector's wall time (every engine call
+    of a sector returns after its device work)."""
     import numpy as np
     p = PATHS[path]
     os.environ.update(p["env"])
@@ -376,6 +378,7 @@ def time_curve(pkg, cfg, path, sectors=None, samples=None):
             for nd in range(n + 1):
                 if sectors is not None and (nu, nd) not in sectors:
                     continue
+                ts = time.perf_counter()
                 info = eng.sector_prepare(nu, nd)
                 blocks = [(k % model.lx, k // model.lx) for k, d in enumerate(info.block_dims) if d > 0]
                 exact = [b for b in blocks if info.block_dims[b[1] * model.lx + b[0]] <= cfg["threshold"]]
@@ -383,6 +386,8 @@ def time_curve(pkg, cfg, path, sectors=None, samples=None):
                 eng.blocks_ftlm_batched([b for b in blocks if b not in exact])
                 for b in blocks:
                     eng.thermo_accumulate_block(*b)
+                if per_sector is not None:
+                    per_sector[(nu, nd)] = time.perf_counter() - ts
         emin, z, ns, n2 = eng.thermo_read()
         secs = time.perf_counter() - t0
     finally:
@@ -426,6 +431,49 @@ def run_curve_reference(args):
                       "e2e": {"value": secs, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
 
 
+def run_curve_per_sector(args, pkg, cfg):
+    """Seconds per n(mu) curve with every sector measured: the mixed batched
+    curve at its full vector count, the FP64 plain path over every sector at
+    --plain-samples vectors (one sweep per vector, so its time is that many
+    vectors' worth; scaled to the full count per sector), and |dn|,
+    |d log Z| of mixed against FP64 batched over the whole curve with the
+    same --dn-samples Philox start vectors on both. Per-sector table to
+    --table (JSON)."""
+    import numpy as np
+    S = cfg["samples"]
+    ps = args.plain_samples or 1
+    ds = args.dn_samples or 8
+    t_mix, t_plain = {}, {}
+    with ClockSampler(0) as clk:
+        tm, _ = time_curve(pkg, cfg, "mixed_batched", per_sector=t_mix)
+        tp, _ = time_curve(pkg, cfg, "fp64_plain", samples=ps, per_sector=t_plain)
+        _, cm = time_curve(pkg, cfg, "mixed_batched", samples=ds)
+        _, cb = time_curve(pkg, cfg, "fp64_batched", samples=ds)
+    rows = []
+    plain_total = 0.0
+    for sec in sorted(t_mix):
+        scaled = t_plain.get(sec, 0.0) * S / ps
+        plain_total += scaled
+        rows.append({"sector": list(sec), "mixed_batched_s": t_mix[sec], "fp64_plain_s_measured": t_plain.get(sec),
+                     "fp64_plain_s_scaled": scaled})
+    line = {"metric": "sec per n(mu) curve", "value": tm, "unit": "s", "n_gpus": 1, "steps": 1, "warmup": 0,
+            "higher_is_better": False, "scaling": "none", "vs_baseline": None,
+            "dtype": "c64 vectors, f64 reductions", "data": "synthetic (model-defined; Philox start vectors)",
+            "config": {"workload": cfg["name"], **{k: v for k, v in cfg.items() if k != "name"}},
+            "curve": {"mixed_batched_s": tm, "fp64_plain_s": plain_total,
+                      "fp64_plain_kind": f"measured on every sector at {ps} of {S} vectors, scaled by {S}/{ps}",
+                      "fp64_plain_s_at_measured_vectors": tp,
+                      "speedup_mixed_batched_vs_fp64_plain": plain_total / tm,
+                      "dn_max_mixed_vs_fp64": float(np.abs(cm["n"] - cb["n"]).max()),
+                      "dlogz_max_mixed_vs_fp64": float(np.abs(cm["log_partition"] - cb["log_partition"]).max()),
+                      "dn_scope": f"whole curve, mixed vs FP64 batched, both with the same {ds} Philox vectors"},
+            "clocks": clk.summary()}
+    if args.table:
+        with open(args.table, "w") as f:
+            json.dump({"line": line, "sectors": rows}, f, indent=1)
+    print(json.dumps(line))
+
+
 def run_curve_mode(args):
     """--curve: seconds per n(mu) curve of the mixed batched path and of the
     FP64 plain path, and |dn|, |d log Z| of mixed against FP64 with the same
@@ -439,6 +487,9 @@ def run_curve_mode(args):
     import ftlm_extended_hubbard_development_b200 as pkg
     cfg = CURVES[args.curve]
     S = cfg["samples"]
+    if args.per_sector:
+        run_curve_per_sector(args, pkg, cfg)
+        return
     with ClockSampler(0) as clk:
         t_mixed, c_mixed = time_curve(pkg, cfg, "mixed_batched")
         if args.plain_sectors:
@@ -488,6 +539,10 @@ def main():
     ap.add_argument("--curve", choices=sorted(CURVES), help="time whole n(mu) curves instead")
     ap.add_argument("--plain-sectors", default="", help="'nu,nd;nu,nd': run the FP64 plain path on these only")
     ap.add_argument("--plain-samples", type=int, default=0)
+    ap.add_argument("--per-sector", action="store_true",
+                    help="--curve: measure every sector (plain path at --plain-samples vectors)")
+    ap.add_argument("--dn-samples", type=int, default=0, help="--per-sector: vectors of the |dn| curves")
+    ap.add_argument("--table", default="", help="--per-sector: write the per-sector table here (JSON)")
     args = ap.parse_args()
     if args.curve:
         if args.impl == "reference":
