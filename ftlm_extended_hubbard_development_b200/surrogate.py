@@ -303,12 +303,18 @@ def heldout_twists(count=8, seed=2024):
 
 def surrogate_twist_average(model: Model, betas, mu, opts: RunOpts, grid=6, heldout=8, dense=24,
                             threshold=0.01, ed=False, epochs=600, seed=2024, levels=LEVELS, members=MEMBERS,
-                            device=0, log=None):
+                            device=0, log=None, judge_opts: RunOpts | None = None):
     """Train on a grid x grid twist set, judge at `heldout` Philox twists with
     the engine, and average n(mu) over the surrogate's dense x dense grid when
     every judge passes (max |dn| <= threshold); otherwise average the
-    engine's own curves at the training and held-out twists (fallback)."""
+    engine's own curves at the training and held-out twists (fallback).
+
+    Two budgets: the training spectra are computed with `opts` (the network's
+    targets are each block's lowest levels, which converge from a few random
+    vectors) and the judges with `judge_opts` (default: the same), the full
+    FTLM budget the surrogate is held to."""
     opts = replace(opts, device=device)
+    judge_opts = replace(judge_opts or opts, device=device)
     t0 = time.perf_counter()
     train = []
     for px, py in uniform_grid(grid):
@@ -326,7 +332,7 @@ def surrogate_twist_average(model: Model, betas, mu, opts: RunOpts, grid=6, held
     t_judge = t_pred = 0.0
     for px, py in heldout_twists(heldout, seed):
         ta = time.perf_counter()
-        td = collect(model, px, py, betas, mu, opts, ed, levels)
+        td = collect(model, px, py, betas, mu, judge_opts, ed, levels)
         tb = time.perf_counter()
         pred = sur.curve(px, py, betas, mu)
         t_judge += tb - ta
@@ -353,6 +359,8 @@ def surrogate_twist_average(model: Model, betas, mu, opts: RunOpts, grid=6, held
     for td in train:
         grid_rows += curve_rows(td.curve, betas, mu)
     timing = {"engine_s_per_twist": (t1 - t0 + t_judge) / max(len(train) + len(judges), 1),
+              "engine_s_per_training_twist": (t1 - t0) / max(len(train), 1),
+              "engine_s_per_judge_twist": t_judge / max(len(judges), 1),
               "training_s": t2 - t1, "surrogate_s_per_twist": t_pred / max(len(judges), 1)}
     return {"average": combine_rows(rows, "observable-average"), "source": source, "accepted": accepted,
             "judges": judges, "loss_history": hist, "training_grid_average": combine_rows(grid_rows),
@@ -382,8 +390,10 @@ def main(argv=None):
     ap.add_argument("--mu-min", type=float, default=-3.0)
     ap.add_argument("--mu-max", type=float, default=4.0)
     ap.add_argument("--mu-points", type=int, default=141)
-    ap.add_argument("--samples", type=int, default=128)
-    ap.add_argument("--lanczos-steps", type=int, default=80)
+    ap.add_argument("--samples", type=int, default=128, help="random vectors of the training spectra")
+    ap.add_argument("--lanczos-steps", type=int, default=80, help="Lanczos steps of the training spectra")
+    ap.add_argument("--judge-samples", type=int, default=0, help="random vectors of the judges (default --samples)")
+    ap.add_argument("--judge-steps", type=int, default=0, help="Lanczos steps of the judges (default --lanczos-steps)")
     ap.add_argument("--exact-block-threshold", type=int, default=256)
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
     ap.add_argument("--start-vector", choices=["ref-gaussian", "philox-phase"], default="philox-phase")
@@ -403,15 +413,18 @@ def main(argv=None):
     opts = RunOpts(samples=a.samples, lanczos_steps=a.lanczos_steps, exact_block_threshold=a.exact_block_threshold,
                    precision=PREC_MIXED if a.precision == "mixed" else PREC_FP64,
                    start_vector=START_PHILOX_PHASE if a.start_vector == "philox-phase" else START_REF_GAUSSIAN)
+    jopts = replace(opts, samples=a.judge_samples or a.samples, lanczos_steps=a.judge_steps or a.lanczos_steps)
     res = surrogate_twist_average(model, betas, mu, opts, grid=a.grid, heldout=a.heldout, dense=a.dense,
                                   threshold=a.threshold, ed=a.ed, epochs=a.epochs, members=a.members,
-                                  device=a.device, log=lambda m: print(m, file=sys.stderr, flush=True))
+                                  device=a.device, log=lambda m: print(m, file=sys.stderr, flush=True),
+                                  judge_opts=jopts)
     es = np.array([j["err_surrogate"] for j in res["judges"]])
     en = np.array([j["err_nearest_twist"] for j in res["judges"]])
     g = np.array([r["n"] for r in res["training_grid_average"]])
     avg = np.array([r["n"] for r in res["average"]])
     print(json.dumps({"model": model.__dict__, "betas": betas, "mu": [a.mu_min, a.mu_max, a.mu_points],
-                      "samples": a.samples, "lanczos_steps": a.lanczos_steps, "ed": a.ed, "grid": a.grid,
+                      "samples": a.samples, "lanczos_steps": a.lanczos_steps,
+                      "judge_samples": jopts.samples, "judge_steps": jopts.lanczos_steps, "ed": a.ed, "grid": a.grid,
                       "heldout": a.heldout, "threshold": a.threshold, "accepted": res["accepted"],
                       "source": res["source"], "judge_max_dn_surrogate": es.round(6).tolist(),
                       "judge_max_dn_nearest_twist": en.round(6).tolist(),
