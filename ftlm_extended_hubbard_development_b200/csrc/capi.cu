@@ -160,6 +160,7 @@ int ftlm_ctx_create(const ftlm_model* model, const ftlm_run_opts* opts, ftlm_ctx
   c.wide = model->lx * model->ly > 32;
   if (const char* hv = std::getenv("FTLM_HV_VARIANT")) c.hv_forced = std::atoi(hv);
   if (const char* rt = std::getenv("FTLM_HV_RETUNE")) c.hv_retune = std::string(rt) == "1";
+  if (const char* sr = std::getenv("FTLM_SEG_ROWS")) c.seg_dynamic = std::string(sr) != "stride";
   if (const char* hm = std::getenv("FTLM_HV_MODE")) {
     const std::string m(hm);
     c.hv_mode = m == "list" ? ftlm::kSrcList : m == "fly" ? ftlm::kSrcFly : m == "split" ? ftlm::kSrcSplit : -1;
@@ -199,7 +200,7 @@ void ftlm_ctx_destroy(ftlm_ctx* ctx) {
                         &c.lz_alpha, &c.lz_beta, &c.lz_scale, &c.lz_state, &c.host_start, &c.ritz_tmp, &c.ritz_out, &c.ritz_meta,
                         &c.sb_rp, &c.sb_col, &c.sb_val, &c.sb_diag, &c.sb_meta, &c.sb_steps,
                         &c.scan_tmp, &c.dense_arena, &c.dense_meta, &c.dense_out, &c.spectra, &c.th_beta,
-                        &c.th_mu, &c.th_state, &c.hl_ptr, &c.hl_ent, &c.flip_map, &c.vec_xd, &c.vec_yd};
+                        &c.th_mu, &c.th_state, &c.hl_ptr, &c.hl_ent, &c.flip_map, &c.vec_xd, &c.vec_yd, &c.seg_counter};
   for (auto* b : bufs) b->release();
   if (c.flipped) {
     ftlm::Ctx& f = *c.flipped;

@@ -187,6 +187,8 @@ struct Ctx {
   int flip_for[4] = {-1, -1, -1, -1};  // (n_up, n_dn, mx, my) the flip map belongs to
   int64_t flip_gen = -1, sec_gen = 0;  // sector generation of the flip map / of the tables
   DBuf vec_xd, vec_yd;  // Lanczos vector and H*V output in the spin-flipped row order
+  bool seg_dynamic = true;  // segment sweeps take rows from a shared counter (FTLM_SEG_ROWS=stride: grid-stride)
+  DBuf seg_counter;         // the row counters of the two sweeps
   bool hv_rows = true;  // narrow sweeps on the hop list: 8 lanes per row (FTLM_HV_ROWS=0: warp per row)
   bool small_blocks = true;  // batched FTLM runs blocks <= kSmallMaxDim in one launch (FTLM_SMALL_BLOCKS=0: off)
   int64_t hl_nnz = 0;

@@ -37,6 +37,8 @@ namespace ftlm {
 
 namespace {
 
+constexpr int kSegGrab = 2;  // rows a warp takes from the shared row counter at a time
+
 int grid_rows(int64_t n, int threads) {
   return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>((n + threads - 1) / threads, 1 << 20)));
 }
@@ -59,7 +61,7 @@ __global__ void __launch_bounds__(kHvThreads, MINB) k_hv_seg(const __grid_consta
                                                            typename CT<T>::V* __restrict__ out,
                                                            const double* __restrict__ scale,
                                                            fx128* __restrict__ partial, const R* __restrict__ gbinom,
-                                                           int with_diag) {
+                                                           int with_diag, unsigned long long* __restrict__ next_row) {
   using V = typename CT<T>::V;
   constexpr int VPL = CT<T>::VPL;
   constexpr int CPR = NV / VPL;
@@ -106,8 +108,25 @@ __global__ void __launch_bounds__(kHvThreads, MINB) k_hv_seg(const __grid_consta
 #pragma unroll
     for (int e = 0; e < VPL; ++e) sc[l][e] = scale ? scale[(l * G + sub) * VPL + e] : 1.0;
 
+  // Rows in order: from a shared counter (next_row, zeroed before the
+  // launch), kSegGrab rows per grab, so all warps stay within a few thousand
+  // consecutive rows and the segment they gather from stays in L2; or
+  // grid-stride when next_row is null. The order does not change any result:
+  // rows are independent and the dot partials are exact integer sums.
   const int64_t nwarps = static_cast<int64_t>(gridDim.x) * kHvWarps;
-  for (int64_t row = static_cast<int64_t>(blockIdx.x) * kHvWarps + wid; row < v.dim; row += nwarps) {
+  int64_t grab = 0, grab_end = 0;
+  int64_t row = static_cast<int64_t>(blockIdx.x) * kHvWarps + wid;
+  while (true) {
+    if (next_row) {
+      if (grab >= grab_end) {
+        unsigned long long r0 = 0;
+        if (lane == 0) r0 = atomicAdd(next_row, static_cast<unsigned long long>(kSegGrab));
+        grab = static_cast<int64_t>(__shfl_sync(0xffffffffu, r0, 0));
+        grab_end = min(grab + kSegGrab, v.dim);
+      }
+      row = grab++;
+    }
+    if (row >= v.dim) break;
     const uint32_t meta = __ldg(v.row_meta + row);
     const uint32_t ur = meta & 0x3FFFFFFu;
     const int deg_s = static_cast<int>(meta >> 26) + 1;
@@ -202,6 +221,7 @@ __global__ void __launch_bounds__(kHvThreads, MINB) k_hv_seg(const __grid_consta
         }
       }
     }
+    if (!next_row) row += nwarps;
   }
   flush_dot<NV>(s_acc, partial);
 }
@@ -262,7 +282,7 @@ __global__ void k_flip_gather_add(int64_t dim, int CPR, typename CT<T>::V* __res
 
 template <typename W, typename R, typename T, int NV, int U, int MINB>
 void launch_seg_t(Ctx& c, Ctx& t, const void* in, void* out, const double* scale, fx128* partial, int grid,
-                  bool with_diag) {
+                  bool with_diag, unsigned long long* next_row) {
   HvParams<W> P;
   P.g = c.geom;
   if constexpr (sizeof(W) == 4) P.v = view32(t);
@@ -270,7 +290,7 @@ void launch_seg_t(Ctx& c, Ctx& t, const void* in, void* out, const double* scale
   using V = typename CT<T>::V;
   const R* gb = sizeof(R) == 4 ? reinterpret_cast<const R*>(c.binom32.p) : reinterpret_cast<const R*>(c.binom.p);
   k_hv_seg<W, R, T, NV, U, MINB><<<grid, kHvThreads, 0, c.stream>>>(P, static_cast<const V*>(in), static_cast<V*>(out),
-                                                                    scale, partial, gb, with_diag ? 1 : 0);
+                                                                    scale, partial, gb, with_diag ? 1 : 0, next_row);
 }
 
 // Variants (gather unroll U, CTAs per SM), as for k_hv; each runs one wave
@@ -281,13 +301,13 @@ constexpr int kSegMinB[kSegVariants] = {4, 4, 3, 2, 2};
 
 template <typename W, typename R, typename T, int NV>
 void launch_seg_var(Ctx& c, Ctx& t, int var, const void* in, void* out, const double* scale, fx128* partial,
-                    int grid, bool with_diag) {
+                    int grid, bool with_diag, unsigned long long* nr) {
   switch (var) {
-    case 0: launch_seg_t<W, R, T, NV, 1, 4>(c, t, in, out, scale, partial, grid, with_diag); return;
-    case 1: launch_seg_t<W, R, T, NV, 2, 4>(c, t, in, out, scale, partial, grid, with_diag); return;
-    case 2: launch_seg_t<W, R, T, NV, 4, 3>(c, t, in, out, scale, partial, grid, with_diag); return;
-    case 3: launch_seg_t<W, R, T, NV, 4, 2>(c, t, in, out, scale, partial, grid, with_diag); return;
-    case 4: launch_seg_t<W, R, T, NV, 8, 2>(c, t, in, out, scale, partial, grid, with_diag); return;
+    case 0: launch_seg_t<W, R, T, NV, 1, 4>(c, t, in, out, scale, partial, grid, with_diag, nr); return;
+    case 1: launch_seg_t<W, R, T, NV, 2, 4>(c, t, in, out, scale, partial, grid, with_diag, nr); return;
+    case 2: launch_seg_t<W, R, T, NV, 4, 3>(c, t, in, out, scale, partial, grid, with_diag, nr); return;
+    case 3: launch_seg_t<W, R, T, NV, 4, 2>(c, t, in, out, scale, partial, grid, with_diag, nr); return;
+    case 4: launch_seg_t<W, R, T, NV, 8, 2>(c, t, in, out, scale, partial, grid, with_diag, nr); return;
     default: break;
   }
   throw Error(FTLM_ERR_ARG, "bad H*V kernel variant");
@@ -295,34 +315,42 @@ void launch_seg_var(Ctx& c, Ctx& t, int var, const void* in, void* out, const do
 
 template <typename W, typename R, typename T>
 void launch_seg_nv(Ctx& c, Ctx& t, int var, const void* in, void* out, int nv, const double* scale, fx128* partial,
-                   int grid, bool with_diag) {
+                   int grid, bool with_diag, unsigned long long* nr) {
   switch (nv) {
     case 1:
       if constexpr (sizeof(T) == 8) {
-        launch_seg_var<W, R, T, 1>(c, t, var, in, out, scale, partial, grid, with_diag);
+        launch_seg_var<W, R, T, 1>(c, t, var, in, out, scale, partial, grid, with_diag, nr);
         return;
       }
       break;
-    case 2: launch_seg_var<W, R, T, 2>(c, t, var, in, out, scale, partial, grid, with_diag); return;
-    case 4: launch_seg_var<W, R, T, 4>(c, t, var, in, out, scale, partial, grid, with_diag); return;
-    case 8: launch_seg_var<W, R, T, 8>(c, t, var, in, out, scale, partial, grid, with_diag); return;
-    case 16: launch_seg_var<W, R, T, 16>(c, t, var, in, out, scale, partial, grid, with_diag); return;
-    case 32: launch_seg_var<W, R, T, 32>(c, t, var, in, out, scale, partial, grid, with_diag); return;
-    case 64: launch_seg_var<W, R, T, 64>(c, t, var, in, out, scale, partial, grid, with_diag); return;
-    case 128: launch_seg_var<W, R, T, 128>(c, t, var, in, out, scale, partial, grid, with_diag); return;
+    case 2: launch_seg_var<W, R, T, 2>(c, t, var, in, out, scale, partial, grid, with_diag, nr); return;
+    case 4: launch_seg_var<W, R, T, 4>(c, t, var, in, out, scale, partial, grid, with_diag, nr); return;
+    case 8: launch_seg_var<W, R, T, 8>(c, t, var, in, out, scale, partial, grid, with_diag, nr); return;
+    case 16: launch_seg_var<W, R, T, 16>(c, t, var, in, out, scale, partial, grid, with_diag, nr); return;
+    case 32: launch_seg_var<W, R, T, 32>(c, t, var, in, out, scale, partial, grid, with_diag, nr); return;
+    case 64: launch_seg_var<W, R, T, 64>(c, t, var, in, out, scale, partial, grid, with_diag, nr); return;
+    case 128: launch_seg_var<W, R, T, 128>(c, t, var, in, out, scale, partial, grid, with_diag, nr); return;
     default: break;
   }
   throw Error(FTLM_ERR_ARG, "unsupported vectors per sweep: " + std::to_string(nv));
 }
 
+// next_row: c.seg_sched's counter for this sweep (zeroed here, on the
+// stream) or null for grid-stride rows.
 void launch_seg(Ctx& c, Ctx& t, int var, const void* in, void* out, int nv, bool fp32, const double* scale,
-                fx128* partial, int grid, bool with_diag) {
+                fx128* partial, int grid, bool with_diag, int counter_slot) {
+  unsigned long long* nr = nullptr;
+  if (c.seg_dynamic) {
+    c.seg_counter.ensure(sizeof(unsigned long long) * 4);
+    nr = c.seg_counter.as<unsigned long long>() + counter_slot;
+    FTLM_CUDA(cudaMemsetAsync(nr, 0, sizeof(unsigned long long), c.stream));
+  }
   if (c.wide) {
-    if (fp32) launch_seg_nv<uint64_t, uint64_t, float>(c, t, var, in, out, nv, scale, partial, grid, with_diag);
-    else launch_seg_nv<uint64_t, uint64_t, double>(c, t, var, in, out, nv, scale, partial, grid, with_diag);
+    if (fp32) launch_seg_nv<uint64_t, uint64_t, float>(c, t, var, in, out, nv, scale, partial, grid, with_diag, nr);
+    else launch_seg_nv<uint64_t, uint64_t, double>(c, t, var, in, out, nv, scale, partial, grid, with_diag, nr);
   } else {
-    if (fp32) launch_seg_nv<uint32_t, uint32_t, float>(c, t, var, in, out, nv, scale, partial, grid, with_diag);
-    else launch_seg_nv<uint32_t, uint32_t, double>(c, t, var, in, out, nv, scale, partial, grid, with_diag);
+    if (fp32) launch_seg_nv<uint32_t, uint32_t, float>(c, t, var, in, out, nv, scale, partial, grid, with_diag, nr);
+    else launch_seg_nv<uint32_t, uint32_t, double>(c, t, var, in, out, nv, scale, partial, grid, with_diag, nr);
   }
   FTLM_LAUNCH_CHECK();
 }
@@ -436,12 +464,12 @@ int seg_variant(Ctx& c, const void* in, void* out, int nv, bool fp32) {
   float best_ms[kSegVariants];
   for (int v = 0; v < kSegVariants; ++v) {
     best_ms[v] = 1e30f;
-    launch_seg(c, c, v, in, out, nv, fp32, nullptr, nullptr, seg_grid(c, v), true);  // warm
+    launch_seg(c, c, v, in, out, nv, fp32, nullptr, nullptr, seg_grid(c, v), true, 0);  // warm
   }
   for (int rep = 0; rep < 3; ++rep)
     for (int v = 0; v < kSegVariants; ++v) {
       FTLM_CUDA(cudaEventRecord(e0, c.stream));
-      launch_seg(c, c, v, in, out, nv, fp32, nullptr, nullptr, seg_grid(c, v), true);
+      launch_seg(c, c, v, in, out, nv, fp32, nullptr, nullptr, seg_grid(c, v), true, 0);
       FTLM_CUDA(cudaEventRecord(e1, c.stream));
       FTLM_CUDA(cudaEventSynchronize(e1));
       float ms = 0.f;
@@ -467,8 +495,8 @@ int hv_apply_split(Ctx& c, const void* in, const void* in_d, void* out, void* ou
   const int grid = seg_grid(c, var);
   // flipped sweep first: its partials follow this block's in the array
   launch_seg(c, f, var, in_d, out_d, nv, fp32, scale, partial ? partial + static_cast<int64_t>(grid) * nv : nullptr,
-             grid, false);
-  launch_seg(c, c, var, in, out, nv, fp32, scale, partial, grid, true);
+             grid, false, 1);
+  launch_seg(c, c, var, in, out, nv, fp32, scale, partial, grid, true, 0);
   c.prof.kernel_launches += 2;
   return 2 * grid;
 }

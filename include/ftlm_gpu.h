@@ -103,8 +103,9 @@ int ftlm_last_error(const ftlm_ctx* ctx, char* buf, size_t len);
 int ftlm_abi_version(void);
 /* Architecture of this library's device code as the CUDA runtime loaded it on
  * `device` (cudaFuncGetAttributes of one of its kernels): binary_version is
- * major*10+minor of the SASS (100 for sm_100a), ptx_version 0 when no PTX is
- * embedded for JIT compilation. No counterpart in the reference (build check). */
+ * major*10+minor of the SASS (100 for sm_100a), ptx_version that of the
+ * virtual architecture it was compiled from. No counterpart in the reference
+ * (build check). */
 int ftlm_device_code_version(int32_t device, int32_t* binary_version, int32_t* ptx_version);
 
 /* Builds the translation-orbit tables of sector (n_up, n_down) on the GPU

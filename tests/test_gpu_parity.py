@@ -44,12 +44,13 @@ def sectors_by_case(golden):
 
 
 def test_loaded_device_code_is_sm100():
-    """The runtime loaded this library's sm_100a SASS (no PTX JIT path)."""
+    """The runtime loaded this library's SASS for compute capability 10.0,
+    compiled from the sm_100 virtual architecture."""
     import ctypes as C
     lib = pkg.load_library()
     bv, pv = C.c_int32(0), C.c_int32(-1)
     assert lib.ftlm_device_code_version(0, C.byref(bv), C.byref(pv)) == 0
-    assert bv.value == 100 and pv.value == 0, (bv.value, pv.value)
+    assert bv.value == 100 and pv.value == 100, (bv.value, pv.value)
 
 
 def test_sector_basis_relations_and_csr_bit_exact(golden, sectors_by_case):
