@@ -189,6 +189,11 @@ struct Ctx {
   DBuf vec_xd, vec_yd;  // Lanczos vector and H*V output in the spin-flipped row order
   bool seg_dynamic = true;  // segment sweeps take rows from a shared counter (FTLM_SEG_ROWS=stride: grid-stride)
   DBuf seg_counter;         // the row counters of the two sweeps
+  bool split_stencil = true;  // segment sweeps read the class stencils (FTLM_SPLIT_OP=fly: on-the-fly lookups)
+  // class stencils of this context's prepared block (split.cu)
+  bool stn_ok = false;
+  int64_t stn_for[3] = {-1, -1, -1};  // (sector generation, mx, my) they belong to
+  DBuf stn_crb, stn_rp, stn_ent, stn_cnt;
   bool hv_rows = true;  // narrow sweeps on the hop list: 8 lanes per row (FTLM_HV_ROWS=0: warp per row)
   bool small_blocks = true;  // batched FTLM runs blocks <= kSmallMaxDim in one launch (FTLM_SMALL_BLOCKS=0: off)
   int64_t hl_nnz = 0;

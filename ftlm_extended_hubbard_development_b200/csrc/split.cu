@@ -226,6 +226,180 @@ __global__ void __launch_bounds__(kHvThreads, MINB) k_hv_seg(const __grid_consta
   flush_dot<NV>(s_acc, partial);
 }
 
+// ---------------------------------------------------------------- stencils
+//
+// Class stencils: within one segment (fixed up representative ur) the
+// down-spin operator depends only on the stabiliser class of ur, not on ur
+// itself. Class 0 (trivial stabiliser) has every down word as a row in rank
+// order; class c > 0 has its active canonical down words (act_list). So the
+// down-spin hops of a whole block are one small CSR per class ("stencil"),
+// rows = class rows, entries = the hop's target index inside the segment
+// (16 bits) | dir << 16 | parity << 19 | shift << 20 | (deg - 1) << 26, in the
+// on-the-fly kernel's hop order (source site ascending, direction ascending;
+// hops to inactive orbits left out). The stencils of a 4x4 half-filled block
+// take about 1 MB and stay in L1/L2, so a sweep reads per row only its row
+// metadata and the gathered rows; the per-row rank and class-table lookups
+// of k_hv_seg are gone. Needs C(N, N_down) <= 65536 (18 sites at half filling).
+
+constexpr int64_t kStencilMaxRows = 65536;
+
+template <typename W>
+__global__ void k_stencil(int fill, const __grid_constant__ Geom g, int nclass, const int64_t* __restrict__ crb,
+                          int64_t c_dn, const uint32_t* __restrict__ act_list, const uint64_t* __restrict__ dtab,
+                          const W* __restrict__ dns, const uint64_t* __restrict__ binom, int64_t rows,
+                          int32_t* __restrict__ counts, const int64_t* __restrict__ rp, uint32_t* __restrict__ ent) {
+  for (int64_t r = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; r < rows;
+       r += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    int lo = 0, hi = nclass - 1;  // class c with crb[c] <= r < crb[c+1]
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) / 2;
+      if (crb[mid] <= r) lo = mid;
+      else hi = mid - 1;
+    }
+    const int c = lo;
+    const int64_t a = r - crb[c];
+    const int64_t j = c == 0 ? a : static_cast<int64_t>(act_list[static_cast<int64_t>(c - 1) * c_dn + a]);
+    const W d = dns[j];
+    int64_t pos = fill ? rp[r] : 0;
+    int cnt = 0;
+    for (W m = d; m; m &= m - 1) {
+      const int from = ctz(m);
+      for (int dir = 0; dir < 8; ++dir) {
+        if (g.amp_re[dir] == 0.0 && g.amp_im[dir] == 0.0) continue;
+        const int to = g.nb[from][dir];
+        if ((d >> to) & 1) continue;
+        const W moved = d ^ (static_cast<W>(1) << from) ^ (static_cast<W>(1) << to);
+        const int64_t rd = static_cast<int64_t>(rank_of<W, uint64_t>(moved, binom));
+        int64_t at = rd;
+        int h = 0, sg = 0, deg = 1;
+        if (c != 0) {
+          const uint64_t e = dtab[static_cast<int64_t>(c - 1) * c_dn + rd];
+          at = static_cast<int32_t>(static_cast<uint32_t>(e));
+          if (at < 0) continue;
+          h = static_cast<int>((e >> 32) & 0xFF);
+          sg = static_cast<int>((e >> 40) & 1);
+          deg = static_cast<int>((e >> 48) & 0xFF);
+        }
+        if (fill)
+          ent[pos++] = static_cast<uint32_t>(at) | (static_cast<uint32_t>(dir) << 16) |
+                       (static_cast<uint32_t>(jw_parity(d, from, to) ^ sg) << 19) | (static_cast<uint32_t>(h) << 20) |
+                       (static_cast<uint32_t>(deg - 1) << 26);
+        ++cnt;
+      }
+    }
+    if (!fill) counts[r] = cnt;
+  }
+}
+
+// The segment sweep (same contract as k_hv_seg) with the class stencils as
+// the operator source.
+template <typename W, typename T, int NV, int U, int MINB>
+__global__ void __launch_bounds__(kHvThreads, MINB) k_hv_stn(const __grid_constant__ HvParams<W> P,
+                                                           const int64_t* __restrict__ crb,
+                                                           const int64_t* __restrict__ srp,
+                                                           const uint32_t* __restrict__ sent,
+                                                           const typename CT<T>::V* __restrict__ in,
+                                                           typename CT<T>::V* __restrict__ out,
+                                                           const double* __restrict__ scale,
+                                                           fx128* __restrict__ partial, int with_diag,
+                                                           unsigned long long* __restrict__ next_row) {
+  using V = typename CT<T>::V;
+  constexpr int VPL = CT<T>::VPL;
+  constexpr int CPR = NV / VPL;
+  constexpr int G = CPR < 32 ? CPR : 32;
+  constexpr int LPL = CPR / G;
+  __shared__ double s_ph[2][64];
+  __shared__ double s_amp[2][8];
+  __shared__ double s_sq[65];
+  __shared__ fx128 s_acc[kHvWarps][NV];
+  const Geom& g = P.g;
+  const BlockView<W>& v = P.v;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < 64; i += kHvThreads) {
+    s_ph[0][i] = v.phase_re[i];
+    s_ph[1][i] = v.phase_im[i];
+  }
+  if (tid < 8) {
+    s_amp[0][tid] = g.amp_re[tid];
+    s_amp[1][tid] = g.amp_im[tid];
+  }
+  if (tid < 65) s_sq[tid] = g.sqrt_deg[tid];
+  for (int i = tid; i < kHvWarps * NV; i += kHvThreads) s_acc[i / NV][i % NV] = 0;
+  __syncthreads();
+  const int lane = tid & 31;
+  const int wid = tid >> 5;
+  const int grp = lane / G;
+  const int sub = lane % G;
+  double sc[LPL][VPL];
+#pragma unroll
+  for (int l = 0; l < LPL; ++l)
+#pragma unroll
+    for (int e = 0; e < VPL; ++e) sc[l][e] = scale ? scale[(l * G + sub) * VPL + e] : 1.0;
+  const int64_t nwarps = static_cast<int64_t>(gridDim.x) * kHvWarps;
+  int64_t grab = 0, grab_end = 0;
+  int64_t row = static_cast<int64_t>(blockIdx.x) * kHvWarps + wid;
+  while (true) {
+    if (next_row) {
+      if (grab >= grab_end) {
+        unsigned long long r0 = 0;
+        if (lane == 0) r0 = atomicAdd(next_row, static_cast<unsigned long long>(kSegGrab));
+        grab = static_cast<int64_t>(__shfl_sync(0xffffffffu, r0, 0));
+        grab_end = min(grab + kSegGrab, v.dim);
+      }
+      row = grab++;
+    }
+    if (row >= v.dim) break;
+    const uint32_t meta = __ldg(v.row_meta + row);
+    const uint32_t ur = meta & 0x3FFFFFFu;
+    const double inv_s = 1.0 / s_sq[static_cast<int>(meta >> 26) + 1];
+    const int64_t seg = __ldg(v.aoff + ur);
+    const int64_t cr = __ldg(crb + __ldg(v.ur_class + ur)) + (row - seg);
+    const int64_t h0 = __ldg(srp + cr), h1 = __ldg(srp + cr + 1);
+    V acc[LPL];
+#pragma unroll
+    for (int l = 0; l < LPL; ++l) vzero(acc[l]);
+    for (int64_t b = h0; b < h1; b += 32) {
+      const int64_t q = b + lane;
+      int64_t col = -1;
+      T cr_ = 0, ci = 0;
+      if (q < h1) {
+        const uint32_t e = __ldg(sent + q);
+        col = seg + static_cast<int64_t>(e & 0xFFFFu);
+        const int dir = static_cast<int>((e >> 16) & 7);
+        const int p = static_cast<int>((e >> 19) & 1);
+        const int shift = static_cast<int>((e >> 20) & 63);
+        const int deg_t = static_cast<int>((e >> 26) & 63) + 1;
+        const double ar = p ? -s_amp[0][dir] : s_amp[0][dir];
+        const double ai = p ? -s_amp[1][dir] : s_amp[1][dir];
+        const double pr = s_ph[0][shift], pi = s_ph[1][shift];
+        const double ratio = s_sq[deg_t] * inv_s;
+        cr_ = static_cast<T>((ar * pr - ai * pi) * ratio);
+        ci = static_cast<T>((ar * pi + ai * pr) * ratio);
+      }
+      gather_batch<T, NV, U>(in, col, cr_, ci, static_cast<int>(min(static_cast<int64_t>(32), h1 - b)), acc);
+    }
+#pragma unroll
+    for (int o = G; o < 32; o <<= 1)
+#pragma unroll
+      for (int l = 0; l < LPL; ++l) vadd(acc[l], shfl_xor_v(acc[l], o));
+    if (grp == 0) {
+      const double diag = with_diag ? diag_energy(__ldg(v.ur_bits + ur), __ldg(v.row_dn + row), g) : 0.0;
+#pragma unroll
+      for (int l = 0; l < LPL; ++l) {
+        const V x = ld_stream(in + row * CPR + l * G + sub);
+        double dt2[VPL];
+        st_stream(out + row * CPR + l * G + sub, finish_row(x, acc[l], diag, sc[l], dt2));
+        if (partial) {
+#pragma unroll
+          for (int e = 0; e < VPL; ++e) s_acc[wid][(l * G + sub) * VPL + e] += fx_of(dt2[e]);
+        }
+      }
+    }
+    if (!next_row) row += nwarps;
+  }
+  flush_dot<NV>(s_acc, partial);
+}
+
 // Flip map of every row q of block Pu: the flipped state (d, u) resolved in
 // the tables vd of sector (N_down, N_up): row p | shift << 32 | sign << 38.
 template <typename W>
@@ -288,6 +462,12 @@ void launch_seg_t(Ctx& c, Ctx& t, const void* in, void* out, const double* scale
   if constexpr (sizeof(W) == 4) P.v = view32(t);
   else P.v = view64(t);
   using V = typename CT<T>::V;
+  if (c.split_stencil && t.stn_ok) {
+    k_hv_stn<W, T, NV, U, MINB><<<grid, kHvThreads, 0, c.stream>>>(
+        P, t.stn_crb.as<int64_t>(), t.stn_rp.as<int64_t>(), t.stn_ent.as<uint32_t>(), static_cast<const V*>(in),
+        static_cast<V*>(out), scale, partial, with_diag ? 1 : 0, next_row);
+    return;
+  }
   const R* gb = sizeof(R) == 4 ? reinterpret_cast<const R*>(c.binom32.p) : reinterpret_cast<const R*>(c.binom.p);
   k_hv_seg<W, R, T, NV, U, MINB><<<grid, kHvThreads, 0, c.stream>>>(P, static_cast<const V*>(in), static_cast<V*>(out),
                                                                     scale, partial, gb, with_diag ? 1 : 0, next_row);
@@ -389,6 +569,48 @@ Ctx& flipped_tables(Ctx& c) {
   return f;
 }
 
+// Class stencils of the prepared block of tables t (its own sector and
+// block); false when a class has more than kStencilMaxRows rows.
+template <typename W>
+bool stencil_build_t(Ctx& c, Ctx& t) {
+  const SectorTables& S = t.sec;
+  const BlockTables& B = t.blk;
+  if (S.c_dn > kStencilMaxRows) return false;
+  std::vector<int64_t> crb(S.nclass + 1, 0);
+  for (int k = 0; k < S.nclass; ++k) crb[k + 1] = crb[k] + (k == 0 ? S.c_dn : B.cls_nact[k]);
+  const int64_t rows = crb[S.nclass];
+  t.stn_crb.ensure(sizeof(int64_t) * (S.nclass + 1));
+  FTLM_CUDA(cudaMemcpyAsync(t.stn_crb.p, crb.data(), sizeof(int64_t) * crb.size(), cudaMemcpyHostToDevice, c.stream));
+  t.stn_cnt.ensure(sizeof(int32_t) * std::max<int64_t>(rows, 1));
+  t.stn_rp.ensure(sizeof(int64_t) * (rows + 1));
+  const int grid = grid_rows(rows, 128);
+  k_stencil<W><<<grid, 128, 0, c.stream>>>(0, c.geom, S.nclass, t.stn_crb.as<int64_t>(), S.c_dn,
+                                           B.act_list.as<uint32_t>(), B.dtab.as<uint64_t>(), S.dns.as<W>(),
+                                           c.binom.as<uint64_t>(), rows, t.stn_cnt.as<int32_t>(), nullptr, nullptr);
+  FTLM_LAUNCH_CHECK();
+  const int64_t total = scan_excl_i32_to_i64(c, t.stn_cnt.as<int32_t>(), t.stn_rp.as<int64_t>(), rows);
+  FTLM_CUDA(cudaMemcpyAsync(t.stn_rp.as<int64_t>() + rows, &total, sizeof(int64_t), cudaMemcpyHostToDevice,
+                            c.stream));
+  t.stn_ent.ensure(sizeof(uint32_t) * std::max<int64_t>(total, 1));
+  k_stencil<W><<<grid, 128, 0, c.stream>>>(1, c.geom, S.nclass, t.stn_crb.as<int64_t>(), S.c_dn,
+                                           B.act_list.as<uint32_t>(), B.dtab.as<uint64_t>(), S.dns.as<W>(),
+                                           c.binom.as<uint64_t>(), rows, nullptr, t.stn_rp.as<int64_t>(),
+                                           t.stn_ent.as<uint32_t>());
+  FTLM_LAUNCH_CHECK();
+  FTLM_CUDA(cudaStreamSynchronize(c.stream));
+  c.prof.kernel_launches += 5;
+  return true;
+}
+
+// Stencils of tables t for its prepared block, built once per (sector
+// generation, block).
+void stencil_prepare(Ctx& c, Ctx& t) {
+  const int64_t key[3] = {t.sec_gen, t.blk.mx, t.blk.my};
+  if (std::memcmp(key, t.stn_for, sizeof key) == 0) return;
+  t.stn_ok = c.wide ? stencil_build_t<uint64_t>(c, t) : stencil_build_t<uint32_t>(c, t);
+  std::memcpy(t.stn_for, key, sizeof key);
+}
+
 template <typename W>
 void flip_map_build_t(Ctx& c, Ctx& f) {
   HvParams<W> P;
@@ -443,6 +665,10 @@ bool split_prepare(Ctx& c, int nv, bool fp32) {
     std::memcpy(c.flip_for, key, sizeof key);
     c.flip_gen = c.sec_gen;
   }
+  if (c.split_stencil) {
+    stencil_prepare(c, c);
+    if (&f != &c) stencil_prepare(c, f);
+  }
   c.vec_xd.ensure(vec);
   c.vec_yd.ensure(vec);
   return true;
@@ -450,7 +676,8 @@ bool split_prepare(Ctx& c, int nv, bool fp32) {
 
 int seg_variant(Ctx& c, const void* in, void* out, int nv, bool fp32) {
   if (c.hv_forced >= 0 && c.hv_forced < kSegVariants) return c.hv_forced;
-  const uint64_t key = static_cast<uint64_t>((c.wide ? 1 : 0) | 4) | (static_cast<uint64_t>(fp32 ? 1 : 0) << 4) |
+  const uint64_t key = static_cast<uint64_t>((c.wide ? 1 : 0) | 4 | (c.split_stencil && c.stn_ok ? 8 : 0)) |
+                       (static_cast<uint64_t>(fp32 ? 1 : 0) << 4) |
                        (static_cast<uint64_t>(nv) << 8) |
                        (static_cast<uint64_t>(hv_size_class(c.blk.dim)) << 20) |
                        (static_cast<uint64_t>(c.device) << 32);

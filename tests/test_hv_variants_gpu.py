@@ -7,10 +7,12 @@ enough (>= 2^15 rows) that the autotuner itself runs.
   the oracle CSR within 1e-13 (FP64) / 2e-6 (FP32 vectors) of max |H x|;
 * cached hop list `k_hv_list` (all variants) and the narrow-sweep row kernel
   `k_hv_rows`: the same bars;
-* split-spin segment sweeps `k_hv_seg` (both row orders, the spin-flip
-  gather/scatter; sector (3,4) has a separate flipped sector (4,3), sector
-  (3,3) is its own): the same bars against the oracle, bit-identical across
-  variants although each variant runs its own grid;
+* split-spin segment sweeps (both row orders, the spin-flip gather/scatter;
+  sector (3,4) has a separate flipped sector (4,3), sector (3,3) is its own),
+  with the class stencils (`k_hv_stn`, mode "split") and with on-the-fly
+  lookups (`k_hv_seg`, mode "splitfly"): the same bars against the oracle,
+  bit-identical across variants although each variant runs its own grid and
+  rows are taken from a shared counter in whatever order the warps get them;
 * Lanczos alpha/beta identical across variants and equal to the oracle's
   Lanczos from the same start vectors (1e-10 FP64 before the horizon).
 
@@ -67,12 +69,21 @@ CASES = [("fly", E.PREC_FP64, 16), ("fly", E.PREC_MIXED, 128), ("fly", E.PREC_FP
          ("fly", E.PREC_MIXED, 8), ("list", E.PREC_FP64, 16), ("list", E.PREC_MIXED, 32),
          ("list", E.PREC_MIXED, 2), ("list", E.PREC_FP64, 1), ("split", E.PREC_FP64, 16),
          ("split", E.PREC_MIXED, 128), ("split", E.PREC_FP64, 128), ("split", E.PREC_MIXED, 16),
-         ("split", E.PREC_MIXED, 2), ("split", E.PREC_FP64, 1)]
+         ("split", E.PREC_MIXED, 2), ("split", E.PREC_FP64, 1), ("splitfly", E.PREC_FP64, 16),
+         ("splitfly", E.PREC_MIXED, 128), ("splitfly", E.PREC_MIXED, 2)]
+
+
+def set_mode(monkeypatch, mode):
+    monkeypatch.setenv("FTLM_HV_MODE", "split" if mode == "splitfly" else mode)
+    if mode == "splitfly":
+        monkeypatch.setenv("FTLM_SPLIT_OP", "fly")
+    else:
+        monkeypatch.delenv("FTLM_SPLIT_OP", raising=False)
 
 
 @pytest.mark.parametrize("mode,prec,nvec", CASES)
 def test_hv_variants_bit_identical_and_match_oracle(golden, csrs, monkeypatch, mode, prec, nvec):
-    monkeypatch.setenv("FTLM_HV_MODE", mode)
+    set_mode(monkeypatch, mode)
     rng = np.random.default_rng(11)
     tol = 1e-13 if prec == E.PREC_FP64 else 2e-6
     rows_kernel = mode == "list" and nvec * (8 if prec == E.PREC_MIXED else 16) == 16
@@ -92,7 +103,7 @@ def test_hv_variants_bit_identical_and_match_oracle(golden, csrs, monkeypatch, m
                 eng.profile_reset()
                 got[var] = eng.block_apply(mx, my, x)
                 prof = eng.profile()
-            assert prof["hv_source"] == {"fly": 0, "list": 1, "split": 2}[mode]
+            assert prof["hv_source"] == {"fly": 0, "list": 1, "split": 2, "splitfly": 2}[mode]
             if var is None and not rows_kernel:
                 assert prof["tune_runs"] == 1, (case, mode, nvec)  # the tuner measured this block
             assert 0 <= prof["hv_variant"] < 5
@@ -126,13 +137,13 @@ def test_hop_list_agrees_with_on_the_fly_on_large_block(golden, csrs, monkeypatc
 
 @pytest.mark.parametrize("mode,prec,batch", [("fly", E.PREC_FP64, 16), ("fly", E.PREC_MIXED, 128),
                                              ("list", E.PREC_FP64, 8), ("split", E.PREC_FP64, 16),
-                                             ("split", E.PREC_MIXED, 128)])
+                                             ("split", E.PREC_MIXED, 128), ("splitfly", E.PREC_FP64, 16)])
 def test_lanczos_variants_identical_and_match_oracle(golden, csrs, monkeypatch, mode, prec, batch):
     """Alpha/beta of every variant bit-identical; against the oracle's
     Lanczos (main.cpp:1027-1060) from the same start vectors: 1e-10 relative
     (FP64) / 1e-5 (FP32 vectors) over the first 12 steps, well before the
     reproducibility horizon of these blocks."""
-    monkeypatch.setenv("FTLM_HV_MODE", mode)
+    set_mode(monkeypatch, mode)
     case, nu, nd, mx, my = BLOCKS[0]
     csr = csrs[BLOCKS[0]]
     m = model_of(golden, case)
@@ -174,13 +185,15 @@ def test_split_lanczos_agrees_with_on_the_fly(golden, monkeypatch, prec, batch, 
         opts = pkg.RunOpts(samples=batch, lanczos_steps=20, exact_block_threshold=0, precision=prec,
                            batch_vectors=batch, start_vector=E.START_PHILOX_PHASE)
         out = {}
-        for mode in ("fly", "split"):
-            monkeypatch.setenv("FTLM_HV_MODE", mode)
+        for mode in ("fly", "split", "splitfly"):
+            set_mode(monkeypatch, mode)
             with pkg.Engine(m, opts) as eng:
                 eng.sector_prepare(nu, nd)
                 out[mode] = eng.block_lanczos(mx, my)
-        (af, bf, sf), (as_, bs, ss) = out["fly"][:3], out["split"][:3]
-        assert np.array_equal(sf, ss)
-        n = 10  # well before the reproducibility horizon
-        assert np.abs(as_[:, :n] - af[:, :n]).max() <= tol * np.abs(af[:, :n]).max(), case
-        assert np.abs(bs[:, :n] - bf[:, :n]).max() <= tol * np.abs(bf[:, :n]).max(), case
+        af, bf, sf = out["fly"][:3]
+        for mode in ("split", "splitfly"):
+            as_, bs, ss = out[mode][:3]
+            assert np.array_equal(sf, ss)
+            n = 10  # well before the reproducibility horizon
+            assert np.abs(as_[:, :n] - af[:, :n]).max() <= tol * np.abs(af[:, :n]).max(), (case, mode)
+            assert np.abs(bs[:, :n] - bf[:, :n]).max() <= tol * np.abs(bf[:, :n]).max(), (case, mode)
