@@ -162,6 +162,7 @@ int ftlm_ctx_create(const ftlm_model* model, const ftlm_run_opts* opts, ftlm_ctx
   if (const char* rt = std::getenv("FTLM_HV_RETUNE")) c.hv_retune = std::string(rt) == "1";
   if (const char* sr = std::getenv("FTLM_SEG_ROWS")) c.seg_dynamic = std::string(sr) != "stride";
   if (const char* so = std::getenv("FTLM_SPLIT_OP")) c.split_stencil = std::string(so) != "fly";
+  if (const char* sr2 = std::getenv("FTLM_STN_ROWS")) c.stn_rows = std::string(sr2) != "0";
   if (const char* hm = std::getenv("FTLM_HV_MODE")) {
     const std::string m(hm);
     c.hv_mode = m == "list" ? ftlm::kSrcList : m == "fly" ? ftlm::kSrcFly : m == "split" ? ftlm::kSrcSplit : -1;

@@ -190,6 +190,7 @@ struct Ctx {
   bool seg_dynamic = true;  // segment sweeps take rows from a shared counter (FTLM_SEG_ROWS=stride: grid-stride)
   DBuf seg_counter;         // the row counters of the two sweeps
   bool split_stencil = true;  // segment sweeps read the class stencils (FTLM_SPLIT_OP=fly: on-the-fly lookups)
+  bool stn_rows = true;       // narrow stencil sweeps run 8 lanes per row (FTLM_STN_ROWS=0: warp per row)
   // class stencils of this context's prepared block (split.cu)
   bool stn_ok = false;
   int64_t stn_for[3] = {-1, -1, -1};  // (sector generation, mx, my) they belong to

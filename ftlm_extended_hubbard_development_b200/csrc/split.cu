@@ -400,6 +400,143 @@ __global__ void __launch_bounds__(kHvThreads, MINB) k_hv_stn(const __grid_consta
   flush_dot<NV>(s_acc, partial);
 }
 
+// Narrow sweeps (rows of at most 4 chunks: <= 8 FP32 / 4 FP64 vectors) on the
+// class stencils: one warp per row leaves the row's dependent loads (meta ->
+// class, offset -> stencil row -> entries -> gathers) exposed, so 8 lanes
+// share a row and a warp works on 4 rows, each lane taking every 8th hop of
+// its row with kStnChunks 16-byte gathers in flight (kStnChunks / CPR hops);
+// shuffles fold the row. Same contract as k_hv_stn; rows are taken 4 at a
+// time from the shared counter.
+constexpr int kStnLanes = 8;
+constexpr int kStnChunks = 4;
+
+template <typename W, typename T, int NV>
+__global__ void __launch_bounds__(kHvThreads, 4) k_hv_stn_rows(const __grid_constant__ HvParams<W> P,
+                                                               const int64_t* __restrict__ crb,
+                                                               const int64_t* __restrict__ srp,
+                                                               const uint32_t* __restrict__ sent,
+                                                               const typename CT<T>::V* __restrict__ in,
+                                                               typename CT<T>::V* __restrict__ out,
+                                                               const double* __restrict__ scale,
+                                                               fx128* __restrict__ partial, int with_diag,
+                                                               unsigned long long* __restrict__ next_row) {
+  using V = typename CT<T>::V;
+  constexpr int VPL = CT<T>::VPL;
+  constexpr int CPR = NV / VPL;
+  static_assert(CPR >= 1 && CPR <= 4, "narrow sweeps only");
+  constexpr int kStnU = kStnChunks / CPR;  // hops in flight per lane
+  constexpr int kRows = 32 / kStnLanes;  // rows per warp
+  __shared__ double s_ph[2][64];
+  __shared__ double s_amp[2][8];
+  __shared__ double s_sq[65];
+  __shared__ fx128 s_acc[kHvWarps * kRows][NV];
+  const Geom& g = P.g;
+  const BlockView<W>& v = P.v;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < 64; i += kHvThreads) {
+    s_ph[0][i] = v.phase_re[i];
+    s_ph[1][i] = v.phase_im[i];
+  }
+  if (tid < 8) {
+    s_amp[0][tid] = g.amp_re[tid];
+    s_amp[1][tid] = g.amp_im[tid];
+  }
+  if (tid < 65) s_sq[tid] = g.sqrt_deg[tid];
+  for (int i = tid; i < kHvWarps * kRows * NV; i += kHvThreads) s_acc[i / NV][i % NV] = 0;
+  __syncthreads();
+  const int lane = tid & 31;
+  const int wid = tid >> 5;
+  const int grp = lane / kStnLanes;
+  const int sub = lane % kStnLanes;
+  double sc[CPR][VPL];
+#pragma unroll
+  for (int l = 0; l < CPR; ++l)
+#pragma unroll
+    for (int e = 0; e < VPL; ++e) sc[l][e] = scale ? scale[l * VPL + e] : 1.0;
+  const int64_t nwarps = static_cast<int64_t>(gridDim.x) * kHvWarps;
+  int64_t rb = (static_cast<int64_t>(blockIdx.x) * kHvWarps + wid) * kRows;
+  while (true) {
+    if (next_row) {
+      unsigned long long r0 = 0;
+      if (lane == 0) r0 = atomicAdd(next_row, static_cast<unsigned long long>(kRows));
+      rb = static_cast<int64_t>(__shfl_sync(0xffffffffu, r0, 0));
+    }
+    if (rb >= v.dim) break;  // warp-uniform
+    const int64_t row = rb + grp;
+    const bool ok = row < v.dim;
+    uint32_t meta = 0;
+    int64_t seg = 0, h0 = 0, h1 = 0;
+    if (ok) {
+      meta = __ldg(v.row_meta + row);
+      const uint32_t ur = meta & 0x3FFFFFFu;
+      seg = __ldg(v.aoff + ur);
+      const int64_t cr = __ldg(crb + __ldg(v.ur_class + ur)) + (row - seg);
+      h0 = __ldg(srp + cr);
+      h1 = __ldg(srp + cr + 1);
+    }
+    const double inv_s = 1.0 / s_sq[static_cast<int>(meta >> 26) + 1];
+    V acc[CPR];
+#pragma unroll
+    for (int l = 0; l < CPR; ++l) vzero(acc[l]);
+    for (int64_t q0 = h0 + sub; q0 < h1; q0 += kStnLanes * kStnU) {
+      uint32_t e[kStnU];
+#pragma unroll
+      for (int u = 0; u < kStnU; ++u) {
+        const int64_t q = q0 + u * kStnLanes;
+        e[u] = q < h1 ? __ldg(sent + q) : 0xFFFFFFFFu;
+      }
+      V x[kStnU][CPR];
+      T cr_[kStnU], ci[kStnU];
+#pragma unroll
+      for (int u = 0; u < kStnU; ++u) {
+        cr_[u] = 0;
+        ci[u] = 0;
+#pragma unroll
+        for (int l = 0; l < CPR; ++l) vzero(x[u][l]);
+        if (e[u] != 0xFFFFFFFFu) {
+          const int64_t col = seg + static_cast<int64_t>(e[u] & 0xFFFFu);
+          const int dir = static_cast<int>((e[u] >> 16) & 7);
+          const int p = static_cast<int>((e[u] >> 19) & 1);
+          const int shift = static_cast<int>((e[u] >> 20) & 63);
+          const int deg_t = static_cast<int>((e[u] >> 26) & 63) + 1;
+          const double ar = p ? -s_amp[0][dir] : s_amp[0][dir];
+          const double ai = p ? -s_amp[1][dir] : s_amp[1][dir];
+          const double pr = s_ph[0][shift], pi = s_ph[1][shift];
+          const double ratio = s_sq[deg_t] * inv_s;
+          cr_[u] = static_cast<T>((ar * pr - ai * pi) * ratio);
+          ci[u] = static_cast<T>((ar * pi + ai * pr) * ratio);
+#pragma unroll
+          for (int l = 0; l < CPR; ++l) x[u][l] = ld_stream(in + col * CPR + l);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kStnU; ++u)
+#pragma unroll
+        for (int l = 0; l < CPR; ++l) cfma<T>(acc[l], cr_[u], ci[u], x[u][l]);
+    }
+#pragma unroll
+    for (int o = kStnLanes / 2; o > 0; o >>= 1)
+#pragma unroll
+      for (int l = 0; l < CPR; ++l) vadd(acc[l], shfl_xor_v(acc[l], o));
+    if (sub == 0 && ok) {
+      const uint32_t ur = meta & 0x3FFFFFFu;
+      const double diag = with_diag ? diag_energy(__ldg(v.ur_bits + ur), __ldg(v.row_dn + row), g) : 0.0;
+#pragma unroll
+      for (int l = 0; l < CPR; ++l) {
+        const V xr = ld_stream(in + row * CPR + l);
+        double dt2[VPL];
+        st_stream(out + row * CPR + l, finish_row(xr, acc[l], diag, sc[l], dt2));
+        if (partial) {
+#pragma unroll
+          for (int e2 = 0; e2 < VPL; ++e2) s_acc[wid * kRows + grp][l * VPL + e2] += fx_of(dt2[e2]);
+        }
+      }
+    }
+    if (!next_row) rb += nwarps * kRows;
+  }
+  flush_dot<NV>(s_acc, partial);
+}
+
 // Flip map of every row q of block Pu: the flipped state (d, u) resolved in
 // the tables vd of sector (N_down, N_up): row p | shift << 32 | sign << 38.
 template <typename W>
@@ -463,6 +600,16 @@ void launch_seg_t(Ctx& c, Ctx& t, const void* in, void* out, const double* scale
   else P.v = view64(t);
   using V = typename CT<T>::V;
   if (c.split_stencil && t.stn_ok) {
+    if constexpr (NV / CT<T>::VPL <= 4) {
+      if (c.stn_rows) {  // narrow rows: 8 lanes per row (no variants: the same kernel for every U, MINB)
+        k_hv_stn_rows<W, T, NV><<<static_cast<int>(std::min<int64_t>(
+                                      (t.blk.dim + 4 * kHvWarps - 1) / (4 * kHvWarps), int64_t(c.sm_count) * 4)),
+                                  kHvThreads, 0, c.stream>>>(
+            P, t.stn_crb.as<int64_t>(), t.stn_rp.as<int64_t>(), t.stn_ent.as<uint32_t>(), static_cast<const V*>(in),
+            static_cast<V*>(out), scale, partial, with_diag ? 1 : 0, next_row);
+        return;
+      }
+    }
     k_hv_stn<W, T, NV, U, MINB><<<grid, kHvThreads, 0, c.stream>>>(
         P, t.stn_crb.as<int64_t>(), t.stn_rp.as<int64_t>(), t.stn_ent.as<uint32_t>(), static_cast<const V*>(in),
         static_cast<V*>(out), scale, partial, with_diag ? 1 : 0, next_row);
@@ -676,6 +823,7 @@ bool split_prepare(Ctx& c, int nv, bool fp32) {
 
 int seg_variant(Ctx& c, const void* in, void* out, int nv, bool fp32) {
   if (c.hv_forced >= 0 && c.hv_forced < kSegVariants) return c.hv_forced;
+  if (c.split_stencil && c.stn_ok && c.stn_rows && (fp32 ? nv / 2 : nv) <= 4) return 0;  // k_hv_stn_rows: no variants
   const uint64_t key = static_cast<uint64_t>((c.wide ? 1 : 0) | 4 | (c.split_stencil && c.stn_ok ? 8 : 0)) |
                        (static_cast<uint64_t>(fp32 ? 1 : 0) << 4) |
                        (static_cast<uint64_t>(nv) << 8) |

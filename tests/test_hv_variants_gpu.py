@@ -69,7 +69,8 @@ CASES = [("fly", E.PREC_FP64, 16), ("fly", E.PREC_MIXED, 128), ("fly", E.PREC_FP
          ("fly", E.PREC_MIXED, 8), ("list", E.PREC_FP64, 16), ("list", E.PREC_MIXED, 32),
          ("list", E.PREC_MIXED, 2), ("list", E.PREC_FP64, 1), ("split", E.PREC_FP64, 16),
          ("split", E.PREC_MIXED, 128), ("split", E.PREC_FP64, 128), ("split", E.PREC_MIXED, 16),
-         ("split", E.PREC_MIXED, 2), ("split", E.PREC_FP64, 1), ("splitfly", E.PREC_FP64, 16),
+         ("split", E.PREC_MIXED, 2), ("split", E.PREC_FP64, 1), ("split", E.PREC_MIXED, 4),
+         ("split", E.PREC_MIXED, 8), ("split", E.PREC_FP64, 4), ("splitfly", E.PREC_FP64, 16),
          ("splitfly", E.PREC_MIXED, 128), ("splitfly", E.PREC_MIXED, 2)]
 
 
@@ -86,7 +87,9 @@ def test_hv_variants_bit_identical_and_match_oracle(golden, csrs, monkeypatch, m
     set_mode(monkeypatch, mode)
     rng = np.random.default_rng(11)
     tol = 1e-13 if prec == E.PREC_FP64 else 2e-6
-    rows_kernel = mode == "list" and nvec * (8 if prec == E.PREC_MIXED else 16) == 16
+    row_bytes = nvec * (8 if prec == E.PREC_MIXED else 16)
+    # the 8-lanes-per-row kernels have no variants to tune
+    rows_kernel = (mode == "list" and row_bytes == 16) or (mode == "split" and max(row_bytes, 16) <= 64)
     for (case, nu, nd, mx, my), csr in csrs.items():
         m = model_of(golden, case)
         x = rng.standard_normal((csr.dim, nvec)) + 1j * rng.standard_normal((csr.dim, nvec))
