@@ -116,13 +116,15 @@ __global__ void __launch_bounds__(kHvThreads, MINB) k_hv_seg(const __grid_consta
   const int64_t nwarps = static_cast<int64_t>(gridDim.x) * kHvWarps;
   int64_t grab = 0, grab_end = 0;
   int64_t row = static_cast<int64_t>(blockIdx.x) * kHvWarps + wid;
+  // lane 0 keeps the next grab in flight while the current rows are processed
+  unsigned long long pend = 0;
+  if (next_row && lane == 0) pend = atomicAdd(next_row, static_cast<unsigned long long>(kSegGrab));
   while (true) {
     if (next_row) {
       if (grab >= grab_end) {
-        unsigned long long r0 = 0;
-        if (lane == 0) r0 = atomicAdd(next_row, static_cast<unsigned long long>(kSegGrab));
-        grab = static_cast<int64_t>(__shfl_sync(0xffffffffu, r0, 0));
+        grab = static_cast<int64_t>(__shfl_sync(0xffffffffu, pend, 0));
         grab_end = min(grab + kSegGrab, v.dim);
+        if (lane == 0 && grab < v.dim) pend = atomicAdd(next_row, static_cast<unsigned long long>(kSegGrab));
       }
       row = grab++;
     }
@@ -338,13 +340,15 @@ __global__ void __launch_bounds__(kHvThreads, MINB) k_hv_stn(const __grid_consta
   const int64_t nwarps = static_cast<int64_t>(gridDim.x) * kHvWarps;
   int64_t grab = 0, grab_end = 0;
   int64_t row = static_cast<int64_t>(blockIdx.x) * kHvWarps + wid;
+  // lane 0 keeps the next grab in flight while the current rows are processed
+  unsigned long long pend = 0;
+  if (next_row && lane == 0) pend = atomicAdd(next_row, static_cast<unsigned long long>(kSegGrab));
   while (true) {
     if (next_row) {
       if (grab >= grab_end) {
-        unsigned long long r0 = 0;
-        if (lane == 0) r0 = atomicAdd(next_row, static_cast<unsigned long long>(kSegGrab));
-        grab = static_cast<int64_t>(__shfl_sync(0xffffffffu, r0, 0));
+        grab = static_cast<int64_t>(__shfl_sync(0xffffffffu, pend, 0));
         grab_end = min(grab + kSegGrab, v.dim);
+        if (lane == 0 && grab < v.dim) pend = atomicAdd(next_row, static_cast<unsigned long long>(kSegGrab));
       }
       row = grab++;
     }
@@ -455,11 +459,12 @@ __global__ void __launch_bounds__(kHvThreads, 4) k_hv_stn_rows(const __grid_cons
     for (int e = 0; e < VPL; ++e) sc[l][e] = scale ? scale[l * VPL + e] : 1.0;
   const int64_t nwarps = static_cast<int64_t>(gridDim.x) * kHvWarps;
   int64_t rb = (static_cast<int64_t>(blockIdx.x) * kHvWarps + wid) * kRows;
+  unsigned long long pend = 0;  // lane 0: the next grab, in flight while this one is processed
+  if (next_row && lane == 0) pend = atomicAdd(next_row, static_cast<unsigned long long>(kRows));
   while (true) {
     if (next_row) {
-      unsigned long long r0 = 0;
-      if (lane == 0) r0 = atomicAdd(next_row, static_cast<unsigned long long>(kRows));
-      rb = static_cast<int64_t>(__shfl_sync(0xffffffffu, r0, 0));
+      rb = static_cast<int64_t>(__shfl_sync(0xffffffffu, pend, 0));
+      if (lane == 0 && rb < v.dim) pend = atomicAdd(next_row, static_cast<unsigned long long>(kRows));
     }
     if (rb >= v.dim) break;  // warp-uniform
     const int64_t row = rb + grp;
