@@ -833,7 +833,15 @@ int hv_select_source(Ctx& c, int nv, bool fp32) {
   c.split_active = false;
   const int64_t D = c.blk.dim;
   int mode = c.hv_mode;
-  if (mode < 0) mode = D >= (1 << 14) && nv <= (fp32 ? 32 : 16) ? kSrcList : (D >= kSplitMinDim ? kSrcSplit : kSrcFly);
+  if (mode < 0) {
+    // measured on a 4x4 (8,8) block (FP32): split-spin sweeps fastest from 4
+    // vectors up (4.6 vs 7.8 ms per H*V at 4, 35 vs 56 at 128; 243 vs 282 ms at
+    // 16 on 6x3 (9,9)), the hop list's row kernel at one chunk per row
+    const bool one_chunk = nv == (fp32 ? 2 : 1);
+    if (D >= kSplitMinDim && !one_chunk) mode = kSrcSplit;
+    else if (D >= (1 << 14) && nv <= (fp32 ? 32 : 16)) mode = kSrcList;
+    else mode = kSrcFly;
+  }
   if (mode == kSrcList && !hoplist_build(c)) mode = c.hv_mode < 0 && D >= kSplitMinDim ? kSrcSplit : kSrcFly;
   if (mode == kSrcSplit && !split_prepare(c, nv, fp32)) mode = kSrcFly;
   c.hl_active = mode == kSrcList;
