@@ -317,7 +317,14 @@ def run_ours(args):
                                          "gather model: D*[nv*s*(1+h_nz) + nv*s + 8]"),
                          "gather_model_bytes_per_launch": model_bytes,
                          "gather_model_gbs": model_bytes / (hv_s / launches) / 1e9,
-                         "traffic": ncu_traffic(args, split)},
+                         "traffic": ncu_traffic(args, split),
+                         **({"l2_gather_gbs": prof["hv_hops"] * (8 if prec == pkg.engine.PREC_MIXED else 16)
+                                             / hv_s / 1e9,
+                             "note": ("split-spin sweeps: every gather is an L2 hit inside the segment being "
+                                      "processed, so HBM carries only the compulsory bytes (ncu: 1.006x); the "
+                                      "sweeps are bound by L2 gather latency and instruction issue (ncu on the "
+                                      "4x4 (5,5) block: 61% issue, 50% of L2 throughput), "
+                                      "profiles/k_hv_stn_4x4_sector55_nv128_mixed_full.md")} if split else {})},
             "rate": {"hop_vector_products_per_s": prof["hv_hops"] / dev_s,
                      "hv_kernel_hop_vector_products_per_s": prof["hv_hops"] / hv_s,
                      "note": "nonzero off-diagonal hops x vectors per second: precision-neutral"},
