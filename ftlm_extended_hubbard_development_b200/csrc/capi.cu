@@ -243,12 +243,10 @@ int ftlm_sector_prepare(ftlm_ctx* ctx, int32_t n_up, int32_t n_down, ftlm_sector
     info.full_dim = static_cast<uint64_t>(c.sec.full_dim);
     info.parents = static_cast<uint64_t>(c.sec.parents);
     info.n_k = n;
-    c.block_dims.assign(n, 0);
-    for (int my = 0; my < c.geom.ly; ++my)
-      for (int mx = 0; mx < c.geom.lx; ++mx) {
-        c.block_dims[my * c.geom.lx + mx] = ftlm::block_dim_only(c, mx, my);
-        info.block_dim[my * c.geom.lx + mx] = static_cast<uint64_t>(c.block_dims[my * c.geom.lx + mx]);
-      }
+    // block dimensions by character counting on the host (no GPU round
+    // trips); block_prepare checks each against its own row count
+    c.block_dims = ftlm::block_dims_by_characters(c, n_up, n_down);
+    for (int k = 0; k < n; ++k) info.block_dim[k] = static_cast<uint64_t>(c.block_dims[k]);
     if (c.timing) {
       FTLM_CUDA(cudaEventRecord(e1, c.stream));
       FTLM_CUDA(cudaEventSynchronize(e1));

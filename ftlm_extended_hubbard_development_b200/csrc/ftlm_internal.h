@@ -234,6 +234,9 @@ struct Ctx {
 void sector_prepare(Ctx& c, int n_up, int n_dn);
 void block_prepare(Ctx& c, int mx, int my);
 int64_t block_dim_only(Ctx& c, int mx, int my);
+// Dimensions of every block k = my*lx + mx of sector (n_up, n_dn) on the host,
+// by character counting: (1/N) sum_s e^{-ik.s} tr_up(T_s) tr_dn(T_s).
+std::vector<int64_t> block_dims_by_characters(Ctx& c, int n_up, int n_dn);
 void debug_parents(Ctx& c, uint64_t* up, uint64_t* dn, int32_t* deg, double* diag);
 void debug_relations(Ctx& c, int32_t* parent, int32_t* shift, int32_t* sign);
 void block_csr(Ctx& c, std::vector<int32_t>& row_ptr, std::vector<int32_t>& col,

@@ -634,6 +634,106 @@ void block_prepare(Ctx& c, int mx, int my) {
   if (c.blk.mx == mx && c.blk.my == my) return;
   if (c.wide) block_prepare_t<uint64_t>(c, mx, my, true);
   else block_prepare_t<uint32_t>(c, mx, my, true);
+  const size_t k = static_cast<size_t>(my * c.geom.lx + mx);
+  if (k < c.block_dims.size() && c.block_dims[k] != c.blk.dim)
+    throw Error(FTLM_ERR_INTERNAL, "block dimension from the orbit tables differs from the character count");
+}
+
+namespace {
+
+// Translation of a spin word on the host, with the parity of reordering its
+// creation operators (the factorised count of the device translate()).
+uint64_t host_translate(uint64_t b, int dx, int dy, const Geom& g, int* parity) {
+  int par = 0;
+  const int lx = g.lx;
+  if (dx) {
+    uint64_t out = 0;
+    const uint64_t rm = g.rowmask;
+    for (int y = 0; y < g.ly; ++y) {
+      uint64_t row = (b >> (y * lx)) & rm;
+      const int ny = __builtin_popcountll(row);
+      const int wy = __builtin_popcountll(row >> (lx - dx));
+      par += wy * (ny - wy);
+      row = ((row << dx) | (row >> (lx - dx))) & rm;
+      out |= row << (y * lx);
+    }
+    b = out;
+  }
+  if (dy) {
+    const int sh = dy * lx;
+    const uint64_t top = b >> (g.n - sh);
+    const int w = __builtin_popcountll(top);
+    par += w * (__builtin_popcountll(b) - w);
+    b = ((b << sh) | top) & g.full;
+  }
+  *parity = par & 1;
+  return b;
+}
+
+// Trace of T_(dx,dy) on the n-particle words of one spin: the sum over the
+// words it fixes (unions of its site cycles) of its sign.
+int64_t fixed_trace(const Geom& g, int n, int dx, int dy) {
+  if (dx == 0 && dy == 0) {
+    unsigned __int128 r = 1;
+    for (int i = 1; i <= n; ++i) r = r * static_cast<unsigned>(g.n - n + i) / static_cast<unsigned>(i);
+    return static_cast<int64_t>(r);
+  }
+  std::vector<uint64_t> cyc;
+  uint64_t seen = 0;
+  int clen = 0;
+  for (int s0 = 0; s0 < g.n; ++s0) {
+    if ((seen >> s0) & 1) continue;
+    uint64_t m = 0;
+    int len = 0;
+    for (int t = s0; !((seen >> t) & 1);) {
+      seen |= 1ULL << t;
+      m |= 1ULL << t;
+      ++len;
+      t = ((t % g.lx + dx) % g.lx) + ((t / g.lx + dy) % g.ly) * g.lx;
+    }
+    cyc.push_back(m);
+    clen = len;  // every cycle of a translation has the same length
+  }
+  if (n % clen) return 0;
+  const int k = n / clen, nc = static_cast<int>(cyc.size());
+  int64_t tr = 0;
+  std::vector<int> pick(k);
+  for (int i = 0; i < k; ++i) pick[i] = i;
+  while (true) {
+    uint64_t w = 0;
+    for (int i = 0; i < k; ++i) w |= cyc[pick[i]];
+    int par = 0;
+    host_translate(w, dx, dy, g, &par);
+    tr += par ? -1 : 1;
+    int i = k - 1;
+    while (i >= 0 && pick[i] == nc - k + i) --i;
+    if (i < 0) break;
+    ++pick[i];
+    for (int j = i + 1; j < k; ++j) pick[j] = pick[j - 1] + 1;
+  }
+  return tr;
+}
+
+}  // namespace
+
+std::vector<int64_t> block_dims_by_characters(Ctx& c, int n_up, int n_dn) {
+  const Geom& g = c.geom;
+  std::vector<int64_t> tr(g.n);
+  for (int s = 0; s < g.n; ++s)
+    tr[s] = fixed_trace(g, n_up, s % g.lx, s / g.lx) * fixed_trace(g, n_dn, s % g.lx, s / g.lx);
+  const double kPi = 3.141592653589793238462643383279502884;
+  std::vector<int64_t> dims(g.n);
+  for (int my = 0; my < g.ly; ++my)
+    for (int mx = 0; mx < g.lx; ++mx) {
+      double re = 0.0;
+      for (int s = 0; s < g.n; ++s)
+        if (tr[s])
+          re += static_cast<double>(tr[s]) *
+                std::cos(2.0 * kPi * (static_cast<double>(mx * (s % g.lx)) / g.lx +
+                                      static_cast<double>(my * (s / g.lx)) / g.ly));
+      dims[my * g.lx + mx] = static_cast<int64_t>(std::llround(re / g.n));
+    }
+  return dims;
 }
 
 int64_t block_dim_only(Ctx& c, int mx, int my) {
