@@ -202,7 +202,7 @@ void ftlm_ctx_destroy(ftlm_ctx* ctx) {
                         &c.lz_alpha, &c.lz_beta, &c.lz_scale, &c.lz_state, &c.host_start, &c.ritz_tmp, &c.ritz_out, &c.ritz_meta,
                         &c.sb_rp, &c.sb_col, &c.sb_val, &c.sb_diag, &c.sb_meta, &c.sb_steps,
                         &c.scan_tmp, &c.dense_arena, &c.dense_meta, &c.dense_out, &c.spectra, &c.th_beta,
-                        &c.th_mu, &c.th_state, &c.hl_ptr, &c.hl_ent, &c.flip_map, &c.vec_xd, &c.vec_yd, &c.seg_counter, &c.stn_crb, &c.stn_rp, &c.stn_ent, &c.stn_cnt};
+                        &c.th_mu, &c.th_state, &c.hl_ptr, &c.hl_ent, &c.flip_map, &c.vec_xd, &c.vec_yd, &c.seg_counter, &c.stn_crb, &c.stn_rp, &c.stn_rp32, &c.stn_ent, &c.stn_cnt};
   for (auto* b : bufs) b->release();
   if (c.flipped) {
     ftlm::Ctx& f = *c.flipped;
@@ -210,7 +210,7 @@ void ftlm_ctx_destroy(ftlm_ctx* ctx) {
                         &f.sec.d_star, &f.sec.d_hs, &f.sec.d_stab, &f.sec.d_chi, &f.sec.d_cidx, &f.sec.canon,
                         &f.sec.tmp_a, &f.sec.tmp_b, &f.sec.tmp_c, &f.sec.tmp_d, &f.sec.tmp_e, &f.blk.act,
                         &f.blk.act_list, &f.blk.aoff, &f.blk.dtab, &f.blk.row_meta, &f.blk.row_dn, &f.scan_tmp,
-                        &f.stn_crb, &f.stn_rp, &f.stn_ent, &f.stn_cnt};
+                        &f.stn_crb, &f.stn_rp, &f.stn_rp32, &f.stn_ent, &f.stn_cnt};
     for (auto* b : fb) b->release();  // binom tables are the owner's
     c.flipped.reset();
   }

@@ -194,7 +194,7 @@ struct Ctx {
   // class stencils of this context's prepared block (split.cu)
   bool stn_ok = false;
   int64_t stn_for[3] = {-1, -1, -1};  // (sector generation, mx, my) they belong to
-  DBuf stn_crb, stn_rp, stn_ent, stn_cnt;
+  DBuf stn_crb, stn_rp, stn_rp32, stn_ent, stn_cnt;
   bool hv_rows = true;  // narrow sweeps on the hop list: 8 lanes per row (FTLM_HV_ROWS=0: warp per row)
   bool small_blocks = true;  // batched FTLM runs blocks <= kSmallMaxDim in one launch (FTLM_SMALL_BLOCKS=0: off)
   int64_t hl_nnz = 0;

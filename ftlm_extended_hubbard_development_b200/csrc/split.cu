@@ -298,7 +298,7 @@ __global__ void k_stencil(int fill, const __grid_constant__ Geom g, int nclass, 
 template <typename W, typename T, int NV, int U, int MINB>
 __global__ void __launch_bounds__(kHvThreads, MINB) k_hv_stn(const __grid_constant__ HvParams<W> P,
                                                            const int64_t* __restrict__ crb,
-                                                           const int64_t* __restrict__ srp,
+                                                           const int32_t* __restrict__ srp,
                                                            const uint32_t* __restrict__ sent,
                                                            const typename CT<T>::V* __restrict__ in,
                                                            typename CT<T>::V* __restrict__ out,
@@ -313,6 +313,7 @@ __global__ void __launch_bounds__(kHvThreads, MINB) k_hv_stn(const __grid_consta
   __shared__ double s_ph[2][64];
   __shared__ double s_amp[2][8];
   __shared__ double s_sq[65];
+  __shared__ double s_sc[NV];  // vector scales, read at the end of a row (keeps registers for gathers)
   __shared__ fx128 s_acc[kHvWarps][NV];
   const Geom& g = P.g;
   const BlockView<W>& v = P.v;
@@ -326,17 +327,13 @@ __global__ void __launch_bounds__(kHvThreads, MINB) k_hv_stn(const __grid_consta
     s_amp[1][tid] = g.amp_im[tid];
   }
   if (tid < 65) s_sq[tid] = g.sqrt_deg[tid];
+  for (int i = tid; i < NV; i += kHvThreads) s_sc[i] = scale ? scale[i] : 1.0;
   for (int i = tid; i < kHvWarps * NV; i += kHvThreads) s_acc[i / NV][i % NV] = 0;
   __syncthreads();
   const int lane = tid & 31;
   const int wid = tid >> 5;
   const int grp = lane / G;
   const int sub = lane % G;
-  double sc[LPL][VPL];
-#pragma unroll
-  for (int l = 0; l < LPL; ++l)
-#pragma unroll
-    for (int e = 0; e < VPL; ++e) sc[l][e] = scale ? scale[(l * G + sub) * VPL + e] : 1.0;
   const int64_t nwarps = static_cast<int64_t>(gridDim.x) * kHvWarps;
   int64_t grab = 0, grab_end = 0;
   int64_t row = static_cast<int64_t>(blockIdx.x) * kHvWarps + wid;
@@ -358,12 +355,12 @@ __global__ void __launch_bounds__(kHvThreads, MINB) k_hv_stn(const __grid_consta
     const double inv_s = 1.0 / s_sq[static_cast<int>(meta >> 26) + 1];
     const int64_t seg = __ldg(v.aoff + ur);
     const int64_t cr = __ldg(crb + __ldg(v.ur_class + ur)) + (row - seg);
-    const int64_t h0 = __ldg(srp + cr), h1 = __ldg(srp + cr + 1);
+    const int h0 = __ldg(srp + cr), h1 = __ldg(srp + cr + 1);
     V acc[LPL];
 #pragma unroll
     for (int l = 0; l < LPL; ++l) vzero(acc[l]);
-    for (int64_t b = h0; b < h1; b += 32) {
-      const int64_t q = b + lane;
+    for (int b = h0; b < h1; b += 32) {
+      const int q = b + lane;
       int64_t col = -1;
       T cr_ = 0, ci = 0;
       if (q < h1) {
@@ -380,7 +377,7 @@ __global__ void __launch_bounds__(kHvThreads, MINB) k_hv_stn(const __grid_consta
         cr_ = static_cast<T>((ar * pr - ai * pi) * ratio);
         ci = static_cast<T>((ar * pi + ai * pr) * ratio);
       }
-      gather_batch<T, NV, U>(in, col, cr_, ci, static_cast<int>(min(static_cast<int64_t>(32), h1 - b)), acc);
+      gather_batch<T, NV, U>(in, col, cr_, ci, min(32, h1 - b), acc);
     }
 #pragma unroll
     for (int o = G; o < 32; o <<= 1)
@@ -391,8 +388,10 @@ __global__ void __launch_bounds__(kHvThreads, MINB) k_hv_stn(const __grid_consta
 #pragma unroll
       for (int l = 0; l < LPL; ++l) {
         const V x = ld_stream(in + row * CPR + l * G + sub);
-        double dt2[VPL];
-        st_stream(out + row * CPR + l * G + sub, finish_row(x, acc[l], diag, sc[l], dt2));
+        double sc[VPL], dt2[VPL];
+#pragma unroll
+        for (int e = 0; e < VPL; ++e) sc[e] = s_sc[(l * G + sub) * VPL + e];
+        st_stream(out + row * CPR + l * G + sub, finish_row(x, acc[l], diag, sc, dt2));
         if (partial) {
 #pragma unroll
           for (int e = 0; e < VPL; ++e) s_acc[wid][(l * G + sub) * VPL + e] += fx_of(dt2[e]);
@@ -417,7 +416,7 @@ constexpr int kStnChunks = 4;
 template <typename W, typename T, int NV>
 __global__ void __launch_bounds__(kHvThreads, 4) k_hv_stn_rows(const __grid_constant__ HvParams<W> P,
                                                                const int64_t* __restrict__ crb,
-                                                               const int64_t* __restrict__ srp,
+                                                               const int32_t* __restrict__ srp,
                                                                const uint32_t* __restrict__ sent,
                                                                const typename CT<T>::V* __restrict__ in,
                                                                typename CT<T>::V* __restrict__ out,
@@ -470,7 +469,8 @@ __global__ void __launch_bounds__(kHvThreads, 4) k_hv_stn_rows(const __grid_cons
     const int64_t row = rb + grp;
     const bool ok = row < v.dim;
     uint32_t meta = 0;
-    int64_t seg = 0, h0 = 0, h1 = 0;
+    int64_t seg = 0;
+    int h0 = 0, h1 = 0;
     if (ok) {
       meta = __ldg(v.row_meta + row);
       const uint32_t ur = meta & 0x3FFFFFFu;
@@ -483,11 +483,11 @@ __global__ void __launch_bounds__(kHvThreads, 4) k_hv_stn_rows(const __grid_cons
     V acc[CPR];
 #pragma unroll
     for (int l = 0; l < CPR; ++l) vzero(acc[l]);
-    for (int64_t q0 = h0 + sub; q0 < h1; q0 += kStnLanes * kStnU) {
+    for (int q0 = h0 + sub; q0 < h1; q0 += kStnLanes * kStnU) {
       uint32_t e[kStnU];
 #pragma unroll
       for (int u = 0; u < kStnU; ++u) {
-        const int64_t q = q0 + u * kStnLanes;
+        const int q = q0 + u * kStnLanes;
         e[u] = q < h1 ? __ldg(sent + q) : 0xFFFFFFFFu;
       }
       V x[kStnU][CPR];
@@ -610,13 +610,13 @@ void launch_seg_t(Ctx& c, Ctx& t, const void* in, void* out, const double* scale
         k_hv_stn_rows<W, T, NV><<<static_cast<int>(std::min<int64_t>(
                                       (t.blk.dim + 4 * kHvWarps - 1) / (4 * kHvWarps), int64_t(c.sm_count) * 4)),
                                   kHvThreads, 0, c.stream>>>(
-            P, t.stn_crb.as<int64_t>(), t.stn_rp.as<int64_t>(), t.stn_ent.as<uint32_t>(), static_cast<const V*>(in),
+            P, t.stn_crb.as<int64_t>(), t.stn_rp32.as<int32_t>(), t.stn_ent.as<uint32_t>(), static_cast<const V*>(in),
             static_cast<V*>(out), scale, partial, with_diag ? 1 : 0, next_row);
         return;
       }
     }
     k_hv_stn<W, T, NV, U, MINB><<<grid, kHvThreads, 0, c.stream>>>(
-        P, t.stn_crb.as<int64_t>(), t.stn_rp.as<int64_t>(), t.stn_ent.as<uint32_t>(), static_cast<const V*>(in),
+        P, t.stn_crb.as<int64_t>(), t.stn_rp32.as<int32_t>(), t.stn_ent.as<uint32_t>(), static_cast<const V*>(in),
         static_cast<V*>(out), scale, partial, with_diag ? 1 : 0, next_row);
     return;
   }
@@ -721,6 +721,12 @@ Ctx& flipped_tables(Ctx& c) {
   return f;
 }
 
+__global__ void k_rp_narrow(const int64_t* __restrict__ in, int32_t* __restrict__ out, int64_t n) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    out[i] = static_cast<int32_t>(in[i]);
+}
+
 // Class stencils of the prepared block of tables t (its own sector and
 // block); false when a class has more than kStencilMaxRows rows.
 template <typename W>
@@ -734,13 +740,14 @@ bool stencil_build_t(Ctx& c, Ctx& t) {
   t.stn_crb.ensure(sizeof(int64_t) * (S.nclass + 1));
   FTLM_CUDA(cudaMemcpyAsync(t.stn_crb.p, crb.data(), sizeof(int64_t) * crb.size(), cudaMemcpyHostToDevice, c.stream));
   t.stn_cnt.ensure(sizeof(int32_t) * std::max<int64_t>(rows, 1));
-  t.stn_rp.ensure(sizeof(int64_t) * (rows + 1));
+  t.stn_rp.ensure(sizeof(int64_t) * (rows + 1));  // int64 scan, narrowed to int32 below
   const int grid = grid_rows(rows, 128);
   k_stencil<W><<<grid, 128, 0, c.stream>>>(0, c.geom, S.nclass, t.stn_crb.as<int64_t>(), S.c_dn,
                                            B.act_list.as<uint32_t>(), B.dtab.as<uint64_t>(), S.dns.as<W>(),
                                            c.binom.as<uint64_t>(), rows, t.stn_cnt.as<int32_t>(), nullptr, nullptr);
   FTLM_LAUNCH_CHECK();
   const int64_t total = scan_excl_i32_to_i64(c, t.stn_cnt.as<int32_t>(), t.stn_rp.as<int64_t>(), rows);
+  if (total > 0x7fffffffLL) return false;  // the sweeps keep 32-bit entry offsets
   FTLM_CUDA(cudaMemcpyAsync(t.stn_rp.as<int64_t>() + rows, &total, sizeof(int64_t), cudaMemcpyHostToDevice,
                             c.stream));
   t.stn_ent.ensure(sizeof(uint32_t) * std::max<int64_t>(total, 1));
@@ -748,9 +755,13 @@ bool stencil_build_t(Ctx& c, Ctx& t) {
                                            B.act_list.as<uint32_t>(), B.dtab.as<uint64_t>(), S.dns.as<W>(),
                                            c.binom.as<uint64_t>(), rows, nullptr, t.stn_rp.as<int64_t>(),
                                            t.stn_ent.as<uint32_t>());
+  // row offsets as int32 for the sweeps (fewer registers per row)
+  t.stn_rp32.ensure(sizeof(int32_t) * (rows + 1));
+  k_rp_narrow<<<grid_rows(rows + 1, 256), 256, 0, c.stream>>>(t.stn_rp.as<int64_t>(), t.stn_rp32.as<int32_t>(),
+                                                             rows + 1);
   FTLM_LAUNCH_CHECK();
   FTLM_CUDA(cudaStreamSynchronize(c.stream));
-  c.prof.kernel_launches += 5;
+  c.prof.kernel_launches += 6;
   return true;
 }
 
