@@ -38,6 +38,7 @@ namespace ftlm {
 namespace {
 
 constexpr int kSegGrab = 2;  // rows a warp takes from the shared row counter at a time
+constexpr int kStnGrab = 4;  // the same for the stencil sweeps
 
 int grid_rows(int64_t n, int threads) {
   return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>((n + threads - 1) / threads, 1 << 20)));
@@ -339,13 +340,21 @@ __global__ void __launch_bounds__(kHvThreads, MINB) k_hv_stn(const __grid_consta
   int64_t row = static_cast<int64_t>(blockIdx.x) * kHvWarps + wid;
   // lane 0 keeps the next grab in flight while the current rows are processed
   unsigned long long pend = 0;
-  if (next_row && lane == 0) pend = atomicAdd(next_row, static_cast<unsigned long long>(kSegGrab));
+  if (next_row && lane == 0) pend = atomicAdd(next_row, static_cast<unsigned long long>(kStnGrab));
+  // Re<s x, y> of the rows of one grab (kStnGrab consecutive rows starting at
+  // a multiple of kStnGrab, always in row order) summed in FP64, then added
+  // to the exact fixed-point accumulator once per grab: deterministic.
+  double gdot[LPL][VPL];
+#pragma unroll
+  for (int l = 0; l < LPL; ++l)
+#pragma unroll
+    for (int e = 0; e < VPL; ++e) gdot[l][e] = 0.0;
   while (true) {
     if (next_row) {
       if (grab >= grab_end) {
         grab = static_cast<int64_t>(__shfl_sync(0xffffffffu, pend, 0));
-        grab_end = min(grab + kSegGrab, v.dim);
-        if (lane == 0 && grab < v.dim) pend = atomicAdd(next_row, static_cast<unsigned long long>(kSegGrab));
+        grab_end = min(grab + kStnGrab, v.dim);
+        if (lane == 0 && grab < v.dim) pend = atomicAdd(next_row, static_cast<unsigned long long>(kStnGrab));
       }
       row = grab++;
     }
@@ -392,10 +401,17 @@ __global__ void __launch_bounds__(kHvThreads, MINB) k_hv_stn(const __grid_consta
 #pragma unroll
         for (int e = 0; e < VPL; ++e) sc[e] = s_sc[(l * G + sub) * VPL + e];
         st_stream(out + row * CPR + l * G + sub, finish_row(x, acc[l], diag, sc, dt2));
-        if (partial) {
 #pragma unroll
-          for (int e = 0; e < VPL; ++e) s_acc[wid][(l * G + sub) * VPL + e] += fx_of(dt2[e]);
-        }
+        for (int e = 0; e < VPL; ++e) gdot[l][e] += dt2[e];
+      }
+      if (partial && (!next_row || grab >= grab_end)) {  // end of a grab (every row when grid-stride)
+#pragma unroll
+        for (int l = 0; l < LPL; ++l)
+#pragma unroll
+          for (int e = 0; e < VPL; ++e) {
+            s_acc[wid][(l * G + sub) * VPL + e] += fx_of(gdot[l][e]);
+            gdot[l][e] = 0.0;
+          }
       }
     }
     if (!next_row) row += nwarps;
