@@ -295,6 +295,21 @@ class TwistSurrogate:
         return curve_from_blocks(self.predict_blocks(phix, phiy), self.model.sites, betas, mu)
 
 
+def save_twist_data(path, data):
+    """TwistData list to a file (pickle of plain tuples, dicts and arrays)."""
+    import pickle
+    with open(path + ".tmp", "wb") as f:
+        pickle.dump([(d.phix, d.phiy, d.blocks, d.curve) for d in data], f)
+    import os
+    os.replace(path + ".tmp", path)
+
+
+def load_twist_data(path):
+    import pickle
+    with open(path, "rb") as f:
+        return [TwistData(px, py, blocks, curve) for px, py, blocks, curve in pickle.load(f)]
+
+
 def heldout_twists(count=8, seed=2024):
     """Held-out judge twists in [0, 1)^2 from a Philox generator of fixed seed."""
     g = np.random.Generator(np.random.Philox(seed))
@@ -303,7 +318,8 @@ def heldout_twists(count=8, seed=2024):
 
 def surrogate_twist_average(model: Model, betas, mu, opts: RunOpts, grid=6, heldout=8, dense=24,
                             threshold=0.01, ed=False, epochs=600, seed=2024, levels=LEVELS, members=MEMBERS,
-                            device=0, log=None, judge_opts: RunOpts | None = None):
+                            device=0, log=None, judge_opts: RunOpts | None = None, train=None,
+                            save_train=None):
     """Train on a grid x grid twist set, judge at `heldout` Philox twists with
     the engine, and average n(mu) over the surrogate's dense x dense grid when
     every judge passes (max |dn| <= threshold); otherwise average the
@@ -316,12 +332,15 @@ def surrogate_twist_average(model: Model, betas, mu, opts: RunOpts, grid=6, held
     opts = replace(opts, device=device)
     judge_opts = replace(judge_opts or opts, device=device)
     t0 = time.perf_counter()
-    train = []
-    for px, py in uniform_grid(grid):
-        train.append(collect(model, px, py, betas, mu, opts, ed, levels))
-        if log:
-            log(f"training twist {len(train)}/{grid * grid} ({px:.4f}, {py:.4f}) "
-                f"at {time.perf_counter() - t0:.1f} s")
+    if train is None:  # else: training spectra given (a run can stop after collecting them)
+        train = []
+        for px, py in uniform_grid(grid):
+            train.append(collect(model, px, py, betas, mu, opts, ed, levels))
+            if log:
+                log(f"training twist {len(train)}/{grid * grid} ({px:.4f}, {py:.4f}) "
+                    f"at {time.perf_counter() - t0:.1f} s")
+            if save_train:
+                save_twist_data(save_train, train)
     t1 = time.perf_counter()
     if log:
         log(f"training the surrogate on {len(train)} twists")
@@ -406,6 +425,9 @@ def main(argv=None):
     ap.add_argument("--members", type=int, default=MEMBERS)
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--output", help="CSV of the twist-averaged curve")
+    ap.add_argument("--save-train", help="write the training spectra here as they are collected")
+    ap.add_argument("--load-train", help="training spectra from an earlier --save-train (skips collecting)")
+    ap.add_argument("--collect-only", action="store_true", help="stop after collecting the training spectra")
     a = ap.parse_args(argv)
     model = Model(lx=a.lx, ly=a.ly, tx=a.tx, ty=a.ty, tp=a.tp, u=a.u, v=a.v)
     betas = [float(b) for b in a.beta_list.split(",")]
@@ -414,10 +436,23 @@ def main(argv=None):
                    precision=PREC_MIXED if a.precision == "mixed" else PREC_FP64,
                    start_vector=START_PHILOX_PHASE if a.start_vector == "philox-phase" else START_REF_GAUSSIAN)
     jopts = replace(opts, samples=a.judge_samples or a.samples, lanczos_steps=a.judge_steps or a.lanczos_steps)
+    log = lambda m: print(m, file=sys.stderr, flush=True)  # noqa: E731
+    if a.collect_only:
+        t0 = time.perf_counter()
+        train = []
+        for px, py in uniform_grid(a.grid):
+            train.append(collect(model, px, py, betas, mu, replace(opts, device=a.device), a.ed))
+            log(f"training twist {len(train)}/{a.grid ** 2} ({px:.4f}, {py:.4f}) at {time.perf_counter() - t0:.1f} s")
+            if a.save_train:
+                save_twist_data(a.save_train, train)
+        print(json.dumps({"collected": len(train), "seconds": time.perf_counter() - t0,
+                          "s_per_twist": (time.perf_counter() - t0) / len(train)}))
+        return 0
+    train = load_twist_data(a.load_train) if a.load_train else None
     res = surrogate_twist_average(model, betas, mu, opts, grid=a.grid, heldout=a.heldout, dense=a.dense,
                                   threshold=a.threshold, ed=a.ed, epochs=a.epochs, members=a.members,
-                                  device=a.device, log=lambda m: print(m, file=sys.stderr, flush=True),
-                                  judge_opts=jopts)
+                                  device=a.device, log=log, judge_opts=jopts, train=train,
+                                  save_train=a.save_train)
     es = np.array([j["err_surrogate"] for j in res["judges"]])
     en = np.array([j["err_nearest_twist"] for j in res["judges"]])
     g = np.array([r["n"] for r in res["training_grid_average"]])

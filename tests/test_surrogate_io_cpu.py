@@ -1,0 +1,23 @@
+"""Training spectra of the twist surrogate survive a save/load round trip
+(a long run can collect them in one job and train in the next)."""
+import numpy as np
+
+from ftlm_extended_hubbard_development_b200 import surrogate as S
+
+
+def test_twist_data_round_trip(tmp_path):
+    rng = np.random.default_rng(0)
+    data = []
+    for i in range(3):
+        blocks = [(4, 4, 0, 1, 8, rng.normal(size=16), rng.random(16), np.arange(16.0), rng.normal(size=2), bool(i % 2))]
+        curve = {"n": rng.random((1, 5)), "log_partition": rng.normal(size=(1, 5))}
+        data.append(S.TwistData(i / 3, 0.5, blocks, curve))
+    p = str(tmp_path / "train.pkl")
+    S.save_twist_data(p, data)
+    back = S.load_twist_data(p)
+    assert len(back) == 3
+    for a, b in zip(data, back):
+        assert (a.phix, a.phiy) == (b.phix, b.phiy)
+        assert np.array_equal(a.curve["n"], b.curve["n"])
+        for x, y in zip(a.blocks[0], b.blocks[0]):
+            assert np.array_equal(np.asarray(x), np.asarray(y))
