@@ -296,18 +296,38 @@ class TwistSurrogate:
 
 
 def save_twist_data(path, data):
-    """TwistData list to a file (pickle of plain tuples, dicts and arrays)."""
-    import pickle
-    with open(path + ".tmp", "wb") as f:
-        pickle.dump([(d.phix, d.phiy, d.blocks, d.curve) for d in data], f)
+    """TwistData list to a compressed .npz: per twist the block quantum
+    numbers, levels (energies FP64; weights, masks FP32), tail log-partitions
+    and exact flags as arrays, and the engine curve."""
+    arrs = {"n": np.array([len(data)])}
+    for i, d in enumerate(data):
+        b = d.blocks
+        arrs[f"{i}/tw"] = np.array([d.phix, d.phiy])
+        arrs[f"{i}/q"] = np.array([x[:5] for x in b], np.int16).reshape(-1, 5)
+        arrs[f"{i}/E"] = np.array([x[5] for x in b], np.float64)
+        arrs[f"{i}/W"] = np.array([x[6] for x in b], np.float64)
+        arrs[f"{i}/M"] = np.array([x[7] for x in b], np.float32)
+        arrs[f"{i}/T"] = np.array([x[8] for x in b], np.float64)
+        arrs[f"{i}/X"] = np.array([x[9] for x in b], np.bool_)
+        for k, v in d.curve.items():
+            arrs[f"{i}/c/{k}"] = np.asarray(v)
+    tmp = path + ".tmp.npz"
+    np.savez_compressed(tmp, **arrs)
     import os
-    os.replace(path + ".tmp", path)
+    os.replace(tmp, path)
 
 
 def load_twist_data(path):
-    import pickle
-    with open(path, "rb") as f:
-        return [TwistData(px, py, blocks, curve) for px, py, blocks, curve in pickle.load(f)]
+    z = np.load(path)
+    out = []
+    for i in range(int(z["n"][0])):
+        q, E, W, M, T, X = (z[f"{i}/{k}"] for k in ("q", "E", "W", "M", "T", "X"))
+        blocks = [(int(q[j, 0]), int(q[j, 1]), int(q[j, 2]), int(q[j, 3]), int(q[j, 4]), E[j], W[j],
+                   M[j].astype(np.float64), T[j], bool(X[j])) for j in range(len(q))]
+        curve = {k.split("/")[-1]: z[k] for k in z.files if k.startswith(f"{i}/c/")}
+        tw = z[f"{i}/tw"]
+        out.append(TwistData(float(tw[0]), float(tw[1]), blocks, curve))
+    return out
 
 
 def heldout_twists(count=8, seed=2024):

@@ -9,15 +9,17 @@ def test_twist_data_round_trip(tmp_path):
     rng = np.random.default_rng(0)
     data = []
     for i in range(3):
-        blocks = [(4, 4, 0, 1, 8, rng.normal(size=16), rng.random(16), np.arange(16.0), rng.normal(size=2), bool(i % 2))]
+        blocks = [(4, 4, k, 1, 8, rng.normal(size=16), rng.random(16), np.arange(16.0), rng.normal(size=2), bool(k % 2))
+                  for k in range(4)]
         curve = {"n": rng.random((1, 5)), "log_partition": rng.normal(size=(1, 5))}
         data.append(S.TwistData(i / 3, 0.5, blocks, curve))
-    p = str(tmp_path / "train.pkl")
+    p = str(tmp_path / "train.npz")
     S.save_twist_data(p, data)
     back = S.load_twist_data(p)
     assert len(back) == 3
     for a, b in zip(data, back):
         assert (a.phix, a.phiy) == (b.phix, b.phiy)
         assert np.array_equal(a.curve["n"], b.curve["n"])
-        for x, y in zip(a.blocks[0], b.blocks[0]):
-            assert np.array_equal(np.asarray(x), np.asarray(y))
+        for ba, bb in zip(a.blocks, b.blocks):
+            for x, y in zip(ba, bb):
+                assert np.array_equal(np.asarray(x), np.asarray(y))
