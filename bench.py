@@ -309,7 +309,8 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "kernel": (["k_hv (on-the-fly multi-vector H*V)", "k_hv_list (cached hop list)",
-                                     "k_hv_seg x2 (split-spin segment sweeps, both row orders)"]
+                                     "k_hv_stn x2 (split-spin segment sweeps on the class stencils, both "
+                                     "row orders; k_hv_stn_rows at <= 4 chunks per row)"]
                                     [prof["hv_source"]] if prof["hv_source"] in (0, 1, 2) else "unknown"),
                          "kernel_variant": prof["hv_variant"],
                          "bytes_per_launch": bytes_per_launch,
@@ -317,6 +318,7 @@ def run_ours(args):
                                          "gather model: D*[nv*s*(1+h_nz) + nv*s + 8]"),
                          "gather_model_bytes_per_launch": model_bytes,
                          "gather_model_gbs": model_bytes / (hv_s / launches) / 1e9,
+                         "gather_model_frac": model_bytes / (hv_s / launches) / 1e9 / peak,
                          "traffic": ncu_traffic(args, split),
                          **({"l2_gather_gbs": prof["hv_hops"] * (8 if prec == pkg.engine.PREC_MIXED else 16)
                                              / hv_s / 1e9,
