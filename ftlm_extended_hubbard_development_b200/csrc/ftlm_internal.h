@@ -233,7 +233,6 @@ struct Ctx {
 // ---- launchers implemented in the .cu files
 void sector_prepare(Ctx& c, int n_up, int n_dn);
 void block_prepare(Ctx& c, int mx, int my);
-int64_t block_dim_only(Ctx& c, int mx, int my);
 // Dimensions of every block k = my*lx + mx of sector (n_up, n_dn) on the host,
 // by character counting: (1/N) sum_s e^{-ik.s} tr_up(T_s) tr_dn(T_s).
 std::vector<int64_t> block_dims_by_characters(Ctx& c, int n_up, int n_dn);

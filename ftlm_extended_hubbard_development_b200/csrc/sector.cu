@@ -736,14 +736,6 @@ std::vector<int64_t> block_dims_by_characters(Ctx& c, int n_up, int n_dn) {
   return dims;
 }
 
-int64_t block_dim_only(Ctx& c, int mx, int my) {
-  c.blk.mx = c.blk.my = -1;
-  if (c.wide) block_prepare_t<uint64_t>(c, mx, my, false);
-  else block_prepare_t<uint32_t>(c, mx, my, false);
-  c.blk.mx = c.blk.my = -1;  // rows not built
-  return c.blk.dim;
-}
-
 template <typename W>
 BlockView<W> make_view(Ctx& c) {
   BlockView<W> v{};
