@@ -526,6 +526,20 @@ void run_ftlm_block(Ctx& c, int n_up, int n_dn, int mx, int my, Spectrum& out, c
   const bool fp32 = c.opts.precision == FTLM_PREC_MIXED;
   int nvmax = c.opts.batch_vectors > 0 ? c.opts.batch_vectors : std::min(R, 128);
   nvmax = std::min(nvmax, 128);
+  if (c.opts.batch_vectors <= 0) {
+    // Vectors per sweep: the widest sweep whose arrays fit on the device with
+    // 2 GiB to spare (wider sweeps cost less per vector at every width
+    // measured); a large block counts the split sweeps' five arrays.
+    size_t free_b = 0, total_b = 0;
+    FTLM_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const size_t have = c.vec_a.cap + c.vec_b.cap + c.vec_h.cap + c.vec_xd.cap + c.vec_yd.cap;
+    const size_t arrays = D >= kSplitMinDim ? 5 : 3;
+    while (nvmax > 1) {
+      const size_t nv = static_cast<size_t>(next_pow2(std::max(nvmax, fp32 ? 2 : 1)));
+      if (arrays * static_cast<size_t>(D) * nv * (fp32 ? 8 : 16) + (size_t(2) << 30) <= free_b + have) break;
+      nvmax = std::max(1, nvmax / 2);
+    }
+  }
   const uint64_t bseed = block_seed(c.opts.seed, n_up, n_dn, mx, my);
   if (alpha_out) {
     alpha_out->assign(static_cast<size_t>(R) * c.opts.lanczos_steps, 0.0);
