@@ -60,7 +60,7 @@ typedef struct ftlm_run_opts {
   uint64_t seed;                  /* --seed */
   int32_t precision;              /* FTLM_PREC_FP64 | FTLM_PREC_MIXED */
   int32_t start_vector;           /* FTLM_START_REF_GAUSSIAN | FTLM_START_PHILOX_PHASE */
-  int32_t batch_vectors;          /* vectors per H*V sweep; 0 = min(samples, 128) */
+  int32_t batch_vectors;          /* vectors per H*V sweep; 0 = min(samples, 128), halved until the sweep's arrays fit in device memory */
   int32_t device;                 /* CUDA device ordinal */
 } ftlm_run_opts;
 
