@@ -336,6 +336,30 @@ def heldout_twists(count=8, seed=2024):
     return [tuple(map(float, t)) for t in g.random((count, 2))]
 
 
+def collect_grid(model: Model, betas, mu, opts: RunOpts, grid, ed=False, levels=LEVELS, train=None,
+                 save_train=None, log=None):
+    """Training spectra at the grid x grid twists in `uniform_grid` order.
+    `train` holds spectra already collected at the first twists of that
+    order (from `load_twist_data`); collection continues after them and,
+    with `save_train`, rewrites the file after every twist, so a job cut
+    off by a time limit loses at most one twist and the next job resumes."""
+    pts = uniform_grid(grid)
+    train = list(train or [])
+    if len(train) > len(pts):
+        raise ValueError(f"{len(train)} training twists given for a {grid}x{grid} grid")
+    for td, (px, py) in zip(train, pts):
+        if abs(td.phix - px) > 1e-12 or abs(td.phiy - py) > 1e-12:
+            raise ValueError(f"training twist ({td.phix}, {td.phiy}) is not grid twist ({px}, {py})")
+    t0 = time.perf_counter()
+    for px, py in pts[len(train):]:
+        train.append(collect(model, px, py, betas, mu, opts, ed, levels))
+        if log:
+            log(f"training twist {len(train)}/{len(pts)} ({px:.4f}, {py:.4f}) at {time.perf_counter() - t0:.1f} s")
+        if save_train:
+            save_twist_data(save_train, train)
+    return train
+
+
 def surrogate_twist_average(model: Model, betas, mu, opts: RunOpts, grid=6, heldout=8, dense=24,
                             threshold=0.01, ed=False, epochs=600, seed=2024, levels=LEVELS, members=MEMBERS,
                             device=0, log=None, judge_opts: RunOpts | None = None, train=None,
@@ -352,15 +376,9 @@ def surrogate_twist_average(model: Model, betas, mu, opts: RunOpts, grid=6, held
     opts = replace(opts, device=device)
     judge_opts = replace(judge_opts or opts, device=device)
     t0 = time.perf_counter()
-    if train is None:  # else: training spectra given (a run can stop after collecting them)
-        train = []
-        for px, py in uniform_grid(grid):
-            train.append(collect(model, px, py, betas, mu, opts, ed, levels))
-            if log:
-                log(f"training twist {len(train)}/{grid * grid} ({px:.4f}, {py:.4f}) "
-                    f"at {time.perf_counter() - t0:.1f} s")
-            if save_train:
-                save_twist_data(save_train, train)
+    # training spectra given (a run can stop after collecting them) are the
+    # first twists of the grid; the rest are collected here
+    train = collect_grid(model, betas, mu, opts, grid, ed, levels, train, save_train, log)
     t1 = time.perf_counter()
     if log:
         log(f"training the surrogate on {len(train)} twists")
@@ -446,7 +464,8 @@ def main(argv=None):
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--output", help="CSV of the twist-averaged curve")
     ap.add_argument("--save-train", help="write the training spectra here as they are collected")
-    ap.add_argument("--load-train", help="training spectra from an earlier --save-train (skips collecting)")
+    ap.add_argument("--load-train", help="training spectra from an earlier --save-train, the first twists of the grid "
+                    "(collection continues after them)")
     ap.add_argument("--collect-only", action="store_true", help="stop after collecting the training spectra")
     a = ap.parse_args(argv)
     model = Model(lx=a.lx, ly=a.ly, tx=a.tx, ty=a.ty, tp=a.tp, u=a.u, v=a.v)
@@ -457,18 +476,16 @@ def main(argv=None):
                    start_vector=START_PHILOX_PHASE if a.start_vector == "philox-phase" else START_REF_GAUSSIAN)
     jopts = replace(opts, samples=a.judge_samples or a.samples, lanczos_steps=a.judge_steps or a.lanczos_steps)
     log = lambda m: print(m, file=sys.stderr, flush=True)  # noqa: E731
+    train = load_twist_data(a.load_train) if a.load_train else None
     if a.collect_only:
         t0 = time.perf_counter()
-        train = []
-        for px, py in uniform_grid(a.grid):
-            train.append(collect(model, px, py, betas, mu, replace(opts, device=a.device), a.ed))
-            log(f"training twist {len(train)}/{a.grid ** 2} ({px:.4f}, {py:.4f}) at {time.perf_counter() - t0:.1f} s")
-            if a.save_train:
-                save_twist_data(a.save_train, train)
-        print(json.dumps({"collected": len(train), "seconds": time.perf_counter() - t0,
-                          "s_per_twist": (time.perf_counter() - t0) / len(train)}))
+        have = len(train or [])
+        train = collect_grid(model, betas, mu, replace(opts, device=a.device), a.grid, a.ed, train=train,
+                             save_train=a.save_train, log=log)
+        new = len(train) - have
+        print(json.dumps({"collected": len(train), "new": new, "seconds": time.perf_counter() - t0,
+                          "s_per_twist": (time.perf_counter() - t0) / max(new, 1)}))
         return 0
-    train = load_twist_data(a.load_train) if a.load_train else None
     res = surrogate_twist_average(model, betas, mu, opts, grid=a.grid, heldout=a.heldout, dense=a.dense,
                                   threshold=a.threshold, ed=a.ed, epochs=a.epochs, members=a.members,
                                   device=a.device, log=log, judge_opts=jopts, train=train,

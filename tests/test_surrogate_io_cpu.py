@@ -1,6 +1,7 @@
 """Training spectra of the twist surrogate survive a save/load round trip
 (a long run can collect them in one job and train in the next)."""
 import numpy as np
+import pytest
 
 from ftlm_extended_hubbard_development_b200 import surrogate as S
 
@@ -23,3 +24,26 @@ def test_twist_data_round_trip(tmp_path):
         for ba, bb in zip(a.blocks, b.blocks):
             for x, y in zip(ba, bb):
                 assert np.array_equal(np.asarray(x), np.asarray(y))
+
+
+def test_collection_resumes_after_the_saved_twists(tmp_path, monkeypatch):
+    """A collection cut off after k twists resumes at twist k + 1 of the grid,
+    and training spectra that are not the grid's first twists are refused."""
+    calls = []
+
+    def fake_collect(model, px, py, betas, mu, opts, ed=False, levels=16):
+        calls.append((px, py))
+        return S.TwistData(px, py, [], {"n": np.full((1, 2), px + py)})
+
+    monkeypatch.setattr(S, "collect", fake_collect)
+    p = str(tmp_path / "train.npz")
+    first = S.collect_grid(None, [5.0], np.zeros(2), None, 2, train=None, save_train=p)
+    assert calls == [(0.0, 0.0), (0.0, 0.5), (0.5, 0.0), (0.5, 0.5)]
+    calls.clear()
+    part = S.load_twist_data(p)[:2]
+    full = S.collect_grid(None, [5.0], np.zeros(2), None, 2, train=part, save_train=p)
+    assert calls == [(0.5, 0.0), (0.5, 0.5)]
+    assert [(t.phix, t.phiy) for t in full] == [(t.phix, t.phiy) for t in first]
+    assert len(S.load_twist_data(p)) == 4
+    with pytest.raises(ValueError):
+        S.collect_grid(None, [5.0], np.zeros(2), None, 3, train=part)
