@@ -358,9 +358,12 @@ CURVES = {
 # H*V; "batched": FP32 vectors with FP64 sums, all vectors of a block in one
 # sweep, small blocks in one persistent launch, hop list where it pays.
 PATHS = {
-    "mixed_batched": dict(precision="mixed", batch=0, env={"FTLM_SMALL_BLOCKS": "1", "FTLM_HV_MODE": "auto"}),
-    "fp64_batched": dict(precision="fp64", batch=0, env={"FTLM_SMALL_BLOCKS": "1", "FTLM_HV_MODE": "auto"}),
-    "fp64_plain": dict(precision="fp64", batch=1, env={"FTLM_SMALL_BLOCKS": "0", "FTLM_HV_MODE": "fly"}),
+    "mixed_batched": dict(precision="mixed", batch=0, defer=True,
+                          env={"FTLM_SMALL_BLOCKS": "1", "FTLM_HV_MODE": "auto"}),
+    "fp64_batched": dict(precision="fp64", batch=0, defer=True,
+                         env={"FTLM_SMALL_BLOCKS": "1", "FTLM_HV_MODE": "auto"}),
+    "fp64_plain": dict(precision="fp64", batch=1, defer=False,
+                       env={"FTLM_SMALL_BLOCKS": "0", "FTLM_HV_MODE": "fly"}),
 }
 
 
@@ -368,7 +371,8 @@ def time_curve(pkg, cfg, path, sectors=None, samples=None, per_sector=None):
     """Wall time of one n(mu) curve through the C ABI (block order of the
     reference), or of the listed sectors only; returns (seconds, observables).
     per_sector (a dict) receives each sector's wall time (every engine call
-    of a sector returns after its device work)."""
+    of a sector returns after its device work; so the batched paths solve
+    their exact blocks sector by sector there, not pooled over the curve)."""
     import numpy as np
     p = PATHS[path]
     os.environ.update(p["env"])
@@ -382,6 +386,8 @@ def time_curve(pkg, cfg, path, sectors=None, samples=None, per_sector=None):
     try:
         t0 = time.perf_counter()
         eng.thermo_configure(cfg["betas"], mu)
+        # batched paths: the exact blocks of all sectors in one dense-solver launch
+        eng.exact_defer(p["defer"] and per_sector is None)
         n = model.sites
         for nu in range(n + 1):
             for nd in range(n + 1):

@@ -203,69 +203,58 @@ __global__ void __launch_bounds__(kEigThreads) k_dense_eig(int nmat, const int32
   }
 }
 
-}  // namespace
+struct DenseItem {
+  int mx, my;
+  int64_t n, aoff, woff;
+};
 
-void run_exact_blocks(Ctx& c, const std::vector<std::pair<int, int>>& blocks) {
-  struct Item {
-    int mx, my;
-    int64_t n, aoff, eoff, woff;
-  };
-  std::vector<Item> items;
-  int64_t asz = 0, wsz = 0;
-  // dimensions first (tables per block are rebuilt below)
+// Dimensions of the listed blocks (empty ones dropped); aoff/woff relative.
+std::vector<DenseItem> dense_items(Ctx& c, const std::vector<std::pair<int, int>>& blocks, int64_t& asz,
+                                   int64_t& wsz) {
+  std::vector<DenseItem> items;
+  asz = wsz = 0;
   for (const auto& b : blocks) {
-    block_prepare(c, b.first, b.second);
-    const int64_t n = c.blk.dim;
+    const int64_t n = c.block_dims.at(static_cast<size_t>(b.second * c.geom.lx + b.first));
     if (n <= 0) continue;
     if (n > kMaxDense) throw Error(FTLM_ERR_CAPACITY, "block too large for the dense exact solver: " + std::to_string(n));
-    items.push_back({b.first, b.second, n, asz, 0, wsz});
+    items.push_back({b.first, b.second, n, asz, wsz});
     asz += n * n;
     wsz += 2 * n;
   }
-  if (items.empty()) return;
-  c.dense_arena.ensure(sizeof(double2) * asz);
-  c.dense_out.ensure(sizeof(double) * wsz);
-  FTLM_CUDA(cudaMemsetAsync(c.dense_arena.p, 0, sizeof(double2) * asz, c.stream));
-  cudaEvent_t e0 = nullptr, e1 = nullptr;
-  if (c.timing) {
-    FTLM_CUDA(cudaEventCreate(&e0));
-    FTLM_CUDA(cudaEventCreate(&e1));
-    FTLM_CUDA(cudaEventRecord(e0, c.stream));
-  }
-  for (Item& it : items) it.eoff = spectra_alloc(c, it.n);
-  for (Item& it : items) {
+  return items;
+}
+
+// Dense Hermitian matrix of every item at arena + aoff (zeroed by the caller).
+void dense_fill(Ctx& c, const std::vector<DenseItem>& items, double2* arena, int64_t abase) {
+  for (const DenseItem& it : items) {
     // the block's rows are built in stream order; the fill reads them before
     // the next block_prepare overwrites them
     block_prepare(c, it.mx, it.my);
-    double2* A = c.dense_arena.as<double2>() + it.aoff;
+    double2* A = arena + abase + it.aoff;
     block_dense_device(c, A);
     const int g2 = static_cast<int>(std::min<int64_t>((it.n * it.n + 255) / 256, 4096));
     k_dense_herm<<<g2, 256, 0, c.stream>>>(it.n, A);
     FTLM_LAUNCH_CHECK();
     c.prof.kernel_launches += 1;
   }
-  if (c.timing) {
-    FTLM_CUDA(cudaEventRecord(e1, c.stream));
-    FTLM_CUDA(cudaEventSynchronize(e1));
-    float ms = 0.f;
-    FTLM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    c.prof.dense_ms += ms;
-    FTLM_CUDA(cudaEventRecord(e0, c.stream));
-  }
-  // largest first; one CTA per matrix
-  std::vector<int32_t> order(items.size()), dims(items.size());
-  std::vector<int64_t> aoff(items.size()), eoff(items.size()), woff(items.size());
-  int64_t nmax = 0;
-  for (size_t i = 0; i < items.size(); ++i) {
-    dims[i] = static_cast<int32_t>(items[i].n);
-    aoff[i] = items[i].aoff;
-    eoff[i] = items[i].eoff;
-    woff[i] = items[i].woff;
-    nmax = std::max(nmax, items[i].n);
+}
+
+// One k_dense_eig launch over matrices (dims, aoff into arena) writing the
+// eigenvalues at evout + eoff; largest matrix first, one CTA per matrix.
+void dense_solve(Ctx& c, const std::vector<int32_t>& dims, const std::vector<int64_t>& aoff,
+                 const std::vector<int64_t>& eoff, double2* arena, double* evout, double* work) {
+  const size_t nb = dims.size();
+  if (nb == 0) return;
+  std::vector<int32_t> order(nb);
+  std::vector<int64_t> woff(nb);
+  int64_t nmax = 0, wtot = 0;
+  for (size_t i = 0; i < nb; ++i) {
+    woff[i] = wtot;
+    wtot += 2 * static_cast<int64_t>(dims[i]);
+    nmax = std::max<int64_t>(nmax, dims[i]);
   }
   std::iota(order.begin(), order.end(), 0);
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return dims[a] > dims[b]; });
-  const size_t nb = items.size();
   const size_t i32bytes = ((sizeof(int32_t) * 2 * nb + 7) / 8) * 8;  // int64 arrays stay 8-byte aligned
   c.dense_meta.ensure(i32bytes + sizeof(int64_t) * 3 * nb);
   int32_t* d_order = c.dense_meta.as<int32_t>();
@@ -283,32 +272,146 @@ void run_exact_blocks(Ctx& c, const std::vector<std::pair<int, int>>& blocks) {
   if (smem > 48 * 1024)
     FTLM_CUDA(cudaFuncSetAttribute(k_dense_eig, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
   const int grid = static_cast<int>(std::min<size_t>(nb, static_cast<size_t>(c.sm_count) * 4));
-  k_dense_eig<<<grid, kEigThreads, smem, c.stream>>>(static_cast<int>(nb), d_order, d_dims, d_aoff,
-                                                     c.dense_arena.as<double2>(), d_eoff, c.spectra.as<double>(),
-                                                     c.dense_out.as<double>(), d_woff);
+  k_dense_eig<<<grid, kEigThreads, smem, c.stream>>>(static_cast<int>(nb), d_order, d_dims, d_aoff, arena, d_eoff,
+                                                     evout, work, d_woff);
   FTLM_LAUNCH_CHECK();
   c.prof.kernel_launches += 1;
-  if (c.timing) {
+}
+
+struct EventTimer {
+  Ctx& c;
+  double& acc;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  EventTimer(Ctx& c_, double& acc_) : c(c_), acc(acc_) {
+    if (!c.timing) return;
+    FTLM_CUDA(cudaEventCreate(&e0));
+    FTLM_CUDA(cudaEventCreate(&e1));
+    FTLM_CUDA(cudaEventRecord(e0, c.stream));
+  }
+  void stop() {
+    if (!e0) return;
     FTLM_CUDA(cudaEventRecord(e1, c.stream));
     FTLM_CUDA(cudaEventSynchronize(e1));
     float ms = 0.f;
     FTLM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    c.prof.eig_ms += ms;
+    acc += ms;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    e0 = e1 = nullptr;
+  }
+  ~EventTimer() {
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+  }
+};
+
+Spectrum exact_spectrum(const Ctx& c, int64_t n, int64_t ev_off) {
+  Spectrum s;
+  s.ev_off = ev_off;
+  s.w_off = -1;
+  s.count = n;
+  s.exact = true;
+  s.prefactor = 1.0;
+  s.particles = c.sec.n_up + c.sec.n_dn;
+  s.dim = n;
+  return s;
+}
+
+}  // namespace
+
+void run_exact_blocks(Ctx& c, const std::vector<std::pair<int, int>>& blocks) {
+  int64_t asz = 0, wsz = 0;
+  const std::vector<DenseItem> items = dense_items(c, blocks, asz, wsz);
+  if (items.empty()) return;
+  c.dense_arena.ensure(sizeof(double2) * asz);
+  c.dense_out.ensure(sizeof(double) * wsz);
+  FTLM_CUDA(cudaMemsetAsync(c.dense_arena.p, 0, sizeof(double2) * asz, c.stream));
+  std::vector<int32_t> dims;
+  std::vector<int64_t> aoff, eoff;
+  for (const DenseItem& it : items) {
+    dims.push_back(static_cast<int32_t>(it.n));
+    aoff.push_back(it.aoff);
+    eoff.push_back(spectra_alloc(c, it.n));
+  }
+  {
+    EventTimer t(c, c.prof.dense_ms);
+    dense_fill(c, items, c.dense_arena.as<double2>(), 0);
+    t.stop();
+  }
+  {
+    EventTimer t(c, c.prof.eig_ms);
+    dense_solve(c, dims, aoff, eoff, c.dense_arena.as<double2>(), c.spectra.as<double>(), c.dense_out.as<double>());
+    t.stop();
   }
   FTLM_CUDA(cudaStreamSynchronize(c.stream));
-  for (const Item& it : items) {
-    Spectrum s;
-    s.ev_off = it.eoff;
-    s.w_off = -1;
-    s.count = it.n;
-    s.exact = true;
-    s.prefactor = 1.0;
-    s.particles = c.sec.n_up + c.sec.n_dn;
-    s.dim = it.n;
-    c.spec[{it.mx, it.my}] = s;
+  for (size_t i = 0; i < items.size(); ++i) c.spec[{items[i].mx, items[i].my}] = exact_spectrum(c, items[i].n, eoff[i]);
+}
+
+void queue_exact_blocks(Ctx& c, const std::vector<std::pair<int, int>>& blocks) {
+  int64_t asz = 0, wsz = 0;
+  std::vector<DenseItem> items = dense_items(c, blocks, asz, wsz);
+  if (items.empty()) return;
+  if (!c.defer_items.empty() && static_cast<int64_t>(sizeof(double2)) * (c.defer_asz + asz) > kDeferPoolBytes)
+    flush_exact(c);
+  const int64_t base = c.defer_asz;
+  c.defer_arena.ensure_keep(sizeof(double2) * (base + asz), c.stream);
+  FTLM_CUDA(cudaMemsetAsync(c.defer_arena.as<double2>() + base, 0, sizeof(double2) * asz, c.stream));
+  {
+    EventTimer t(c, c.prof.dense_ms);
+    dense_fill(c, items, c.defer_arena.as<double2>(), base);
+    t.stop();
   }
+  c.defer_asz = base + asz;
+  for (const DenseItem& it : items) {
+    Spectrum s = exact_spectrum(c, it.n, -1);
+    s.pending = static_cast<int>(c.defer_items.size());
+    c.spec[{it.mx, it.my}] = s;
+    c.defer_items.push_back({c.sec.n_up, c.sec.n_dn, it.mx, it.my, it.n, base + it.aoff, c.sec_gen});
+  }
+}
+
+void flush_exact(Ctx& c) {
+  if (c.defer_items.empty()) {
+    c.defer_acc.clear();
+    return;
+  }
+  const size_t nb = c.defer_items.size();
+  std::vector<int32_t> dims(nb);
+  std::vector<int64_t> aoff(nb), eoff(nb);
+  int64_t etot = 0;
+  for (size_t i = 0; i < nb; ++i) {
+    dims[i] = static_cast<int32_t>(c.defer_items[i].n);
+    aoff[i] = c.defer_items[i].aoff;
+    eoff[i] = etot;
+    etot += c.defer_items[i].n;
+  }
+  c.defer_ev.ensure(sizeof(double) * etot);
+  c.defer_work.ensure(sizeof(double) * 2 * etot);
+  {
+    EventTimer t(c, c.prof.eig_ms);
+    dense_solve(c, dims, aoff, eoff, c.defer_arena.as<double2>(), c.defer_ev.as<double>(), c.defer_work.as<double>());
+    t.stop();
+  }
+  for (int i : c.defer_acc) {
+    const DeferItem& d = c.defer_items[static_cast<size_t>(i)];
+    thermo_accumulate_dev(c, c.defer_ev.as<double>() + eoff[static_cast<size_t>(i)], nullptr, d.n, 1.0,
+                          d.n_up + d.n_dn);
+  }
+  // pending spectra of the current sector become ordinary exact spectra
+  for (size_t i = 0; i < nb; ++i) {
+    const DeferItem& d = c.defer_items[i];
+    if (d.sec_gen != c.sec_gen) continue;
+    auto it = c.spec.find({d.mx, d.my});
+    if (it == c.spec.end() || it->second.pending != static_cast<int>(i)) continue;
+    const int64_t off = spectra_alloc(c, d.n);
+    FTLM_CUDA(cudaMemcpyAsync(c.spectra.as<double>() + off, c.defer_ev.as<double>() + eoff[i], sizeof(double) * d.n,
+                              cudaMemcpyDeviceToDevice, c.stream));
+    it->second.ev_off = off;
+    it->second.pending = -1;
+  }
+  c.defer_items.clear();
+  c.defer_acc.clear();
+  c.defer_asz = 0;
 }
 
 }  // namespace ftlm

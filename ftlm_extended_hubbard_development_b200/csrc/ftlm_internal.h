@@ -137,6 +137,14 @@ struct Spectrum {
   double prefactor = 1.0;
   int particles = 0;
   int64_t dim = 0;
+  int pending = -1;  // exact block queued for a deferred solve: index into Ctx::defer_items
+};
+
+// An exact block whose dense matrix waits in the deferred pool.
+struct DeferItem {
+  int n_up, n_dn, mx, my;
+  int64_t n, aoff;   // dimension, offset (complex entries) of its matrix in defer_arena
+  int64_t sec_gen;   // sector generation it was assembled in
 };
 
 struct Profile {
@@ -213,6 +221,14 @@ struct Ctx {
   DBuf ritz_tmp, ritz_out, ritz_meta, scan_tmp;
   // exact batch
   DBuf dense_arena, dense_meta, dense_out;
+  // deferred exact blocks (ftlm_exact_defer): matrices of any number of
+  // sectors, diagonalised together by flush_exact; queued accumulations are
+  // indices into defer_items
+  bool exact_defer = false;
+  DBuf defer_arena, defer_ev, defer_work;
+  int64_t defer_asz = 0;
+  std::vector<DeferItem> defer_items;
+  std::vector<int> defer_acc;
   // small-block FTLM batch: CSR arenas, task list, per-vector step counts
   DBuf sb_rp, sb_col, sb_val, sb_diag, sb_meta, sb_steps;
   // spectra of the current sector's blocks (device arena)
@@ -312,10 +328,21 @@ struct RitzJob {
 void ritz_stage_many(Ctx& c, std::vector<RitzJob>& jobs);
 // Exact spectra of several blocks of the prepared sector (one batched launch).
 void run_exact_blocks(Ctx& c, const std::vector<std::pair<int, int>>& blocks);
+// Deferred form: assembles the blocks' matrices into the pool (flushing it
+// first when they would push it past kDeferPoolBytes) and registers them as
+// pending spectra of the current sector.
+void queue_exact_blocks(Ctx& c, const std::vector<std::pair<int, int>>& blocks);
+// Diagonalises every pooled matrix in one launch, runs the queued
+// accumulations in queue order and turns the current sector's pending
+// spectra into ordinary ones; empties the pool.
+void flush_exact(Ctx& c);
+constexpr int64_t kDeferPoolBytes = int64_t(4) << 30;
 // Thermo
 void thermo_configure(Ctx& c, int nbeta, const double* beta, int nmu, const double* mu);
 void thermo_accumulate(Ctx& c, const Spectrum& s);
 void thermo_accumulate_host(Ctx& c, const double* ev, const double* w, int64_t count, double pref, int particles);
+// Accumulates a spectrum already on the device (w null: unit weights).
+void thermo_accumulate_dev(Ctx& c, const double* ev, const double* w, int64_t count, double pref, int particles);
 void thermo_read(Ctx& c, double* emin, double* z, double* n, double* n2);
 
 // Seeds and reference start vectors (main.cpp:514-533, 1015-1025)

@@ -123,6 +123,10 @@ void thermo_accumulate(Ctx& c, const Spectrum& s) {
   launch(c, base + s.ev_off, s.w_off >= 0 ? base + s.w_off : nullptr, s.count, s.prefactor, s.particles);
 }
 
+void thermo_accumulate_dev(Ctx& c, const double* ev, const double* w, int64_t count, double pref, int particles) {
+  launch(c, ev, w, count, pref, particles);
+}
+
 void thermo_accumulate_host(Ctx& c, const double* ev, const double* w, int64_t count, double pref, int particles) {
   if (count <= 0) return;
   DBuf& tmp = c.host_start;
