@@ -394,12 +394,13 @@ def surrogate_twist_average(model: Model, betas, mu, opts: RunOpts, grid=6, held
         pred = sur.curve(px, py, betas, mu)
         t_judge += tb - ta
         t_pred += time.perf_counter() - tb
-        if log:
-            log(f"judge twist ({px:.4f}, {py:.4f}): engine {tb - ta:.1f} s")
         near = sur.nearest(px, py, wrap=True)  # the curve without the network
         judges.append({"twist": (px, py), "curve": td.curve,
                        "err_surrogate": float(np.abs(pred["n"] - td.curve["n"]).max()),
                        "err_nearest_twist": float(np.abs(near.curve["n"] - td.curve["n"]).max())})
+        if log:
+            log(f"judge twist ({px:.4f}, {py:.4f}): engine {tb - ta:.1f} s, max|dn| surrogate "
+                f"{judges[-1]['err_surrogate']:.5f}, nearest training twist {judges[-1]['err_nearest_twist']:.5f}")
     accepted = all(j["err_surrogate"] <= threshold for j in judges)
     rows = []
     if accepted:
