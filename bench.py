@@ -367,12 +367,13 @@ PATHS = {
 }
 
 
-def time_curve(pkg, cfg, path, sectors=None, samples=None, per_sector=None):
+def time_curve(pkg, cfg, path, sectors=None, samples=None, per_sector=None, per_sector_tables=None):
     """Wall time of one n(mu) curve through the C ABI (block order of the
     reference), or of the listed sectors only; returns (seconds, observables).
     per_sector (a dict) receives each sector's wall time (every engine call
     of a sector returns after its device work; so the batched paths solve
-    their exact blocks sector by sector there, not pooled over the curve)."""
+    their exact blocks sector by sector there, not pooled over the curve);
+    per_sector_tables receives the part of it spent in sector_prepare."""
     import numpy as np
     p = PATHS[path]
     os.environ.update(p["env"])
@@ -395,6 +396,8 @@ def time_curve(pkg, cfg, path, sectors=None, samples=None, per_sector=None):
                     continue
                 ts = time.perf_counter()
                 info = eng.sector_prepare(nu, nd)
+                if per_sector_tables is not None:
+                    per_sector_tables[(nu, nd)] = time.perf_counter() - ts
                 blocks = [(k % model.lx, k // model.lx) for k, d in enumerate(info.block_dims) if d > 0]
                 exact = [b for b in blocks if info.block_dims[b[1] * model.lx + b[0]] <= cfg["threshold"]]
                 eng.blocks_exact_batched(exact)
@@ -453,36 +456,50 @@ def run_curve_per_sector(args, pkg, cfg):
     vectors' worth; scaled to the full count per sector), and |dn|,
     |d log Z| of mixed against FP64 batched over the whole curve with the
     same --dn-samples Philox start vectors on both. Per-sector table to
-    --table (JSON)."""
+    --table (JSON). A sector's plain time is scaled as tables + (rest) x
+    vectors / --plain-samples: the sector tables are built once whatever the
+    vector count. --mixed-seconds S takes the mixed curve's time from an
+    earlier whole-curve run instead of measuring it (no per-sector mixed
+    column then); --dn-samples -1 skips the |dn| curves."""
     import numpy as np
     S = cfg["samples"]
     ps = args.plain_samples or 1
     ds = args.dn_samples or 8
-    t_mix, t_plain = {}, {}
+    t_mix, t_plain, t_tab = {}, {}, {}
     with ClockSampler(0) as clk:
-        tm, _ = time_curve(pkg, cfg, "mixed_batched", per_sector=t_mix)
-        tp, _ = time_curve(pkg, cfg, "fp64_plain", samples=ps, per_sector=t_plain)
-        _, cm = time_curve(pkg, cfg, "mixed_batched", samples=ds)
-        _, cb = time_curve(pkg, cfg, "fp64_batched", samples=ds)
+        if args.mixed_seconds > 0:
+            tm = args.mixed_seconds
+        else:
+            tm, _ = time_curve(pkg, cfg, "mixed_batched", per_sector=t_mix)
+        tp, _ = time_curve(pkg, cfg, "fp64_plain", samples=ps, per_sector=t_plain, per_sector_tables=t_tab)
+        if ds > 0:
+            _, cm = time_curve(pkg, cfg, "mixed_batched", samples=ds)
+            _, cb = time_curve(pkg, cfg, "fp64_batched", samples=ds)
     rows = []
     plain_total = 0.0
-    for sec in sorted(t_mix):
-        scaled = t_plain.get(sec, 0.0) * S / ps
+    for sec in sorted(t_plain):
+        scaled = t_tab[sec] + (t_plain[sec] - t_tab[sec]) * S / ps
         plain_total += scaled
-        rows.append({"sector": list(sec), "mixed_batched_s": t_mix[sec], "fp64_plain_s_measured": t_plain.get(sec),
-                     "fp64_plain_s_scaled": scaled})
+        rows.append({"sector": list(sec), "mixed_batched_s": t_mix.get(sec), "fp64_plain_s_measured": t_plain[sec],
+                     "fp64_plain_tables_s": t_tab[sec], "fp64_plain_s_scaled": scaled})
     line = {"metric": "sec per n(mu) curve", "value": tm, "unit": "s", "n_gpus": 1, "steps": 1, "warmup": 0,
             "higher_is_better": False, "scaling": "none", "vs_baseline": None,
             "dtype": "c64 vectors, f64 reductions", "data": "synthetic (model-defined; Philox start vectors)",
             "config": {"workload": cfg["name"], **{k: v for k, v in cfg.items() if k != "name"}},
-            "curve": {"mixed_batched_s": tm, "fp64_plain_s": plain_total,
-                      "fp64_plain_kind": f"measured on every sector at {ps} of {S} vectors, scaled by {S}/{ps}",
+            "curve": {"mixed_batched_s": tm,
+                      "mixed_batched_kind": ("given (--mixed-seconds, an earlier whole-curve run)"
+                                             if args.mixed_seconds > 0 else "measured"),
+                      "fp64_plain_s": plain_total,
+                      "fp64_plain_kind": (f"measured on every sector at {ps} of {S} vectors; per sector tables + "
+                                          f"rest x {S}/{ps}"),
                       "fp64_plain_s_at_measured_vectors": tp,
-                      "speedup_mixed_batched_vs_fp64_plain": plain_total / tm,
-                      "dn_max_mixed_vs_fp64": float(np.abs(cm["n"] - cb["n"]).max()),
-                      "dlogz_max_mixed_vs_fp64": float(np.abs(cm["log_partition"] - cb["log_partition"]).max()),
-                      "dn_scope": f"whole curve, mixed vs FP64 batched, both with the same {ds} Philox vectors"},
+                      "speedup_mixed_batched_vs_fp64_plain": plain_total / tm},
             "clocks": clk.summary()}
+    if ds > 0:
+        line["curve"].update({
+            "dn_max_mixed_vs_fp64": float(np.abs(cm["n"] - cb["n"]).max()),
+            "dlogz_max_mixed_vs_fp64": float(np.abs(cm["log_partition"] - cb["log_partition"]).max()),
+            "dn_scope": f"whole curve, mixed vs FP64 batched, both with the same {ds} Philox vectors"})
     if args.table:
         with open(args.table, "w") as f:
             json.dump({"line": line, "sectors": rows}, f, indent=1)
@@ -556,7 +573,10 @@ def main():
     ap.add_argument("--plain-samples", type=int, default=0)
     ap.add_argument("--per-sector", action="store_true",
                     help="--curve: measure every sector (plain path at --plain-samples vectors)")
-    ap.add_argument("--dn-samples", type=int, default=0, help="--per-sector: vectors of the |dn| curves")
+    ap.add_argument("--dn-samples", type=int, default=0,
+                    help="--per-sector: vectors of the |dn| curves (default 8; -1 skips them)")
+    ap.add_argument("--mixed-seconds", type=float, default=0.0,
+                    help="--per-sector: the mixed curve's seconds from an earlier whole-curve run (skips it)")
     ap.add_argument("--table", default="", help="--per-sector: write the per-sector table here (JSON)")
     args = ap.parse_args()
     if args.curve:
