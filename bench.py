@@ -449,6 +449,54 @@ def run_curve_reference(args):
                       "e2e": {"value": secs, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
 
 
+def run_curve_phases(args, pkg, cfg, reps=2):
+    """--curve ... --phases: the mixed batched curve `reps` times in one
+    process with the engine's profile counters on (CUDA events around each
+    engine call, so slightly slower than the timed curve): host seconds per
+    call kind and the device milliseconds of each phase, one JSON line per
+    repetition; the first repetition pays the process's one-time costs."""
+    p = PATHS["mixed_batched"]
+    os.environ.update(p["env"])
+    model = pkg.Model(**cfg["model"])
+    opts = pkg.RunOpts(samples=cfg["samples"], lanczos_steps=cfg["steps"], exact_block_threshold=cfg["threshold"],
+                       precision=pkg.engine.PREC_MIXED, start_vector=pkg.engine.START_PHILOX_PHASE, batch_vectors=0)
+    mu = pkg.linspace(*cfg["mu"])
+    keys = ("sector_ms", "dense_ms", "eig_ms", "block_ms", "small_ms", "thermo_ms", "kernel_launches")
+    for rep in range(reps):
+        split = dict.fromkeys(("sector_prepare", "exact", "ftlm", "thermo", "flush_and_read"), 0.0)
+        with pkg.Engine(model, opts) as eng:
+            eng.profile(True)
+            eng.profile_reset()
+            t0 = time.perf_counter()
+            eng.thermo_configure(cfg["betas"], mu)
+            eng.exact_defer(True)
+            for nu in range(model.sites + 1):
+                for nd in range(model.sites + 1):
+                    ta = time.perf_counter()
+                    info = eng.sector_prepare(nu, nd)
+                    tb = time.perf_counter()
+                    blocks = [(k % model.lx, k // model.lx) for k, d in enumerate(info.block_dims) if d > 0]
+                    exact = [b for b in blocks if info.block_dims[b[1] * model.lx + b[0]] <= cfg["threshold"]]
+                    eng.blocks_exact_batched(exact)
+                    tc = time.perf_counter()
+                    eng.blocks_ftlm_batched([b for b in blocks if b not in exact])
+                    td = time.perf_counter()
+                    for b in blocks:
+                        eng.thermo_accumulate_block(*b)
+                    te = time.perf_counter()
+                    split["sector_prepare"] += tb - ta
+                    split["exact"] += tc - tb
+                    split["ftlm"] += td - tc
+                    split["thermo"] += te - td
+            tf = time.perf_counter()
+            eng.thermo_read()  # solves the pooled exact blocks, then the queued sums
+            split["flush_and_read"] = time.perf_counter() - tf
+            total = time.perf_counter() - t0
+            prof = eng.profile()
+        print(json.dumps({"rep": rep, "workload": cfg["name"], "total_s": total, "host_split_s": split,
+                          "profile": {k: prof[k] for k in keys}}))
+
+
 def run_curve_per_sector(args, pkg, cfg):
     """Seconds per n(mu) curve with every sector measured: the mixed batched
     curve at its full vector count, the FP64 plain path over every sector at
@@ -519,6 +567,9 @@ def run_curve_mode(args):
     import ftlm_extended_hubbard_development_b200 as pkg
     cfg = CURVES[args.curve]
     S = cfg["samples"]
+    if args.phases:
+        run_curve_phases(args, pkg, cfg)
+        return
     if args.per_sector:
         run_curve_per_sector(args, pkg, cfg)
         return
@@ -577,6 +628,8 @@ def main():
                     help="--per-sector: vectors of the |dn| curves (default 8; -1 skips them)")
     ap.add_argument("--mixed-seconds", type=float, default=0.0,
                     help="--per-sector: the mixed curve's seconds from an earlier whole-curve run (skips it)")
+    ap.add_argument("--phases", action="store_true",
+                    help="--curve: per-phase breakdown of the mixed batched curve (profile counters on)")
     ap.add_argument("--table", default="", help="--per-sector: write the per-sector table here (JSON)")
     args = ap.parse_args()
     if args.curve:
