@@ -372,7 +372,7 @@ def time_curve(pkg, cfg, path, sectors=None, samples=None, per_sector=None, per_
     reference), or of the listed sectors only; returns (seconds, observables).
     per_sector (a dict) receives each sector's wall time (every engine call
     of a sector returns after its device work; so the batched paths solve
-    their exact blocks sector by sector there, not pooled over the curve);
+    their small blocks sector by sector there, not pooled over the curve);
     per_sector_tables receives the part of it spent in sector_prepare."""
     import numpy as np
     p = PATHS[path]
@@ -387,8 +387,8 @@ def time_curve(pkg, cfg, path, sectors=None, samples=None, per_sector=None, per_
     try:
         t0 = time.perf_counter()
         eng.thermo_configure(cfg["betas"], mu)
-        # batched paths: the exact blocks of all sectors in one dense-solver launch
-        eng.exact_defer(p["defer"] and per_sector is None)
+        # batched paths: the small blocks of all sectors in one dense-solver and one Ritz launch
+        eng.spectra_defer(p["defer"] and per_sector is None)
         n = model.sites
         for nu in range(n + 1):
             for nd in range(n + 1):
@@ -469,7 +469,7 @@ def run_curve_phases(args, pkg, cfg, reps=2):
             eng.profile_reset()
             t0 = time.perf_counter()
             eng.thermo_configure(cfg["betas"], mu)
-            eng.exact_defer(True)
+            eng.spectra_defer(True)
             for nu in range(model.sites + 1):
                 for nd in range(model.sites + 1):
                     ta = time.perf_counter()
@@ -489,7 +489,7 @@ def run_curve_phases(args, pkg, cfg, reps=2):
                     split["ftlm"] += td - tc
                     split["thermo"] += te - td
             tf = time.perf_counter()
-            eng.thermo_read()  # solves the pooled exact blocks, then the queued sums
+            eng.thermo_read()  # solves the pooled blocks, then the queued sums
             split["flush_and_read"] = time.perf_counter() - tf
             total = time.perf_counter() - t0
             prof = eng.profile()

@@ -203,7 +203,7 @@ void ftlm_ctx_destroy(ftlm_ctx* ctx) {
                         &c.sb_rp, &c.sb_col, &c.sb_val, &c.sb_diag, &c.sb_meta, &c.sb_steps,
                         &c.scan_tmp, &c.dense_arena, &c.dense_meta, &c.dense_out, &c.spectra, &c.th_beta,
                         &c.th_mu, &c.th_state, &c.hl_ptr, &c.hl_ent, &c.flip_map, &c.vec_xd, &c.vec_yd, &c.seg_counter, &c.stn_crb, &c.stn_rp, &c.stn_rp32, &c.stn_ent, &c.stn_cnt,
-                        &c.defer_arena, &c.defer_ev, &c.defer_work};
+                        &c.defer_arena, &c.defer_ev, &c.defer_work, &c.defer_ab, &c.defer_st};
   for (auto* b : bufs) b->release();
   if (c.flipped) {
     ftlm::Ctx& f = *c.flipped;
@@ -274,20 +274,20 @@ int ftlm_blocks_exact_batched(ftlm_ctx* ctx, const int32_t* mx, const int32_t* m
       ftlm::check_k(c, mx[i], my[i]);
       list.emplace_back(mx[i], my[i]);
     }
-    if (c.exact_defer) ftlm::queue_exact_blocks(c, list);
+    if (c.spectra_defer) ftlm::queue_exact_blocks(c, list);
     else ftlm::run_exact_blocks(c, list);
   });
 }
 
-int ftlm_exact_defer(ftlm_ctx* ctx, int32_t on) {
+int ftlm_spectra_defer(ftlm_ctx* ctx, int32_t on) {
   return ftlm::guarded(ctx, [&](Ctx& c) {
-    if (!on) ftlm::flush_exact(c);
-    c.exact_defer = on != 0;
+    if (!on) ftlm::flush_deferred(c);
+    c.spectra_defer = on != 0;
   });
 }
 
-int ftlm_exact_flush(ftlm_ctx* ctx) {
-  return ftlm::guarded(ctx, [&](Ctx& c) { ftlm::flush_exact(c); });
+int ftlm_spectra_flush(ftlm_ctx* ctx) {
+  return ftlm::guarded(ctx, [&](Ctx& c) { ftlm::flush_deferred(c); });
 }
 
 int ftlm_blocks_ftlm_batched(ftlm_ctx* ctx, const int32_t* mx, const int32_t* my, int32_t nblocks) {
@@ -334,8 +334,8 @@ int ftlm_block_spectrum(ftlm_ctx* ctx, int32_t mx, int32_t my, int32_t exact, do
     const auto key = std::make_pair(static_cast<int>(mx), static_cast<int>(my));
     auto it = c.spec.find(key);
     const bool have = it != c.spec.end() && it->second.exact == (exact != 0);
-    if (have && it->second.pending >= 0) {  // queued for the deferred solve: solve the pool now
-      ftlm::flush_exact(c);
+    if (have && (it->second.pending >= 0 || it->second.pending_ritz >= 0)) {  // pooled: solve the pool now
+      ftlm::flush_deferred(c);
       it = c.spec.find(key);
     }
     if (!have) {
@@ -391,7 +391,7 @@ int ftlm_thermo_configure(ftlm_ctx* ctx, int32_t nbeta, const double* betas, int
     if (nbeta <= 0 || nmu <= 0 || !betas || !mu) throw Error(FTLM_ERR_ARG, "bad beta/mu grid");
     for (int i = 0; i < nbeta; ++i)
       if (!(betas[i] > 0.0)) throw Error(FTLM_ERR_ARG, "All beta values must be positive.");
-    ftlm::flush_exact(c);  // queued accumulations belong to the previous grid
+    ftlm::flush_deferred(c);  // queued accumulations belong to the previous grid
     ftlm::thermo_configure(c, nbeta, betas, nmu, mu);
   });
 }
@@ -402,9 +402,10 @@ int ftlm_thermo_accumulate_block(ftlm_ctx* ctx, int32_t mx, int32_t my) {
     ftlm::check_k(c, mx, my);
     auto it = c.spec.find({mx, my});
     if (it == c.spec.end()) throw Error(FTLM_ERR_STATE, "block spectrum not computed");
-    if (it->second.pending >= 0) {  // accumulated when the pool is solved
+    if (it->second.pending >= 0 || it->second.pending_ritz >= 0) {  // accumulated when the pool is solved
       if (c.nbeta <= 0 || c.nmu <= 0) throw Error(FTLM_ERR_STATE, "thermo accumulators not configured");
-      c.defer_acc.push_back(it->second.pending);
+      const bool ritz = it->second.pending_ritz >= 0;
+      c.defer_acc.push_back({ritz, ritz ? it->second.pending_ritz : it->second.pending});
       return;
     }
     ftlm::thermo_accumulate(c, it->second);
@@ -423,7 +424,7 @@ int ftlm_thermo_read(ftlm_ctx* ctx, double* emin, double* z, double* n, double* 
   return ftlm::guarded(ctx, [&](Ctx& c) {
     if (!emin || !z || !n || !n2) throw Error(FTLM_ERR_ARG, "null output");
     if (c.nbeta <= 0) throw Error(FTLM_ERR_STATE, "thermo accumulators not configured");
-    ftlm::flush_exact(c);
+    ftlm::flush_deferred(c);
     ftlm::thermo_read(c, emin, z, n, n2);
   });
 }

@@ -351,8 +351,8 @@ void queue_exact_blocks(Ctx& c, const std::vector<std::pair<int, int>>& blocks) 
   int64_t asz = 0, wsz = 0;
   std::vector<DenseItem> items = dense_items(c, blocks, asz, wsz);
   if (items.empty()) return;
-  if (!c.defer_items.empty() && static_cast<int64_t>(sizeof(double2)) * (c.defer_asz + asz) > kDeferPoolBytes)
-    flush_exact(c);
+  if (defer_pool_bytes(c) > 0 && defer_pool_bytes(c) + static_cast<int64_t>(sizeof(double2)) * asz > kDeferPoolBytes)
+    flush_deferred(c);
   const int64_t base = c.defer_asz;
   c.defer_arena.ensure_keep(sizeof(double2) * (base + asz), c.stream);
   FTLM_CUDA(cudaMemsetAsync(c.defer_arena.as<double2>() + base, 0, sizeof(double2) * asz, c.stream));
@@ -370,34 +370,64 @@ void queue_exact_blocks(Ctx& c, const std::vector<std::pair<int, int>>& blocks) 
   }
 }
 
-void flush_exact(Ctx& c) {
-  if (c.defer_items.empty()) {
+int64_t defer_pool_bytes(const Ctx& c) {
+  return static_cast<int64_t>(sizeof(double2)) * c.defer_asz + static_cast<int64_t>(sizeof(double)) * c.defer_ab_used +
+         static_cast<int64_t>(sizeof(int32_t)) * c.defer_st_used;
+}
+
+void flush_deferred(Ctx& c) {
+  const size_t nb = c.defer_items.size();
+  const size_t nr = c.defer_ritz.size();
+  if (nb == 0 && nr == 0) {
     c.defer_acc.clear();
     return;
   }
-  const size_t nb = c.defer_items.size();
-  std::vector<int32_t> dims(nb);
-  std::vector<int64_t> aoff(nb), eoff(nb);
-  int64_t etot = 0;
-  for (size_t i = 0; i < nb; ++i) {
-    dims[i] = static_cast<int32_t>(c.defer_items[i].n);
-    aoff[i] = c.defer_items[i].aoff;
-    eoff[i] = etot;
-    etot += c.defer_items[i].n;
-  }
-  c.defer_ev.ensure(sizeof(double) * etot);
-  c.defer_work.ensure(sizeof(double) * 2 * etot);
-  {
+  // exact blocks: one dense-solver launch
+  std::vector<int64_t> eoff(nb);
+  if (nb > 0) {
+    std::vector<int32_t> dims(nb);
+    std::vector<int64_t> aoff(nb);
+    int64_t etot = 0;
+    for (size_t i = 0; i < nb; ++i) {
+      dims[i] = static_cast<int32_t>(c.defer_items[i].n);
+      aoff[i] = c.defer_items[i].aoff;
+      eoff[i] = etot;
+      etot += c.defer_items[i].n;
+    }
+    c.defer_ev.ensure(sizeof(double) * etot);
+    c.defer_work.ensure(sizeof(double) * 2 * etot);
     EventTimer t(c, c.prof.eig_ms);
     dense_solve(c, dims, aoff, eoff, c.defer_arena.as<double2>(), c.defer_ev.as<double>(), c.defer_work.as<double>());
     t.stop();
   }
-  for (int i : c.defer_acc) {
-    const DeferItem& d = c.defer_items[static_cast<size_t>(i)];
-    thermo_accumulate_dev(c, c.defer_ev.as<double>() + eoff[static_cast<size_t>(i)], nullptr, d.n, 1.0,
-                          d.n_up + d.n_dn);
+  // small FTLM blocks: one Ritz-stage launch; the spectra land in this
+  // sector's arena (those of earlier sectors are dropped with it later)
+  std::vector<Spectrum> rs(nr);
+  if (nr > 0) {
+    std::vector<RitzJob> jobs;
+    jobs.reserve(nr);
+    for (size_t i = 0; i < nr; ++i) {
+      const DeferRitz& d = c.defer_ritz[i];
+      jobs.push_back(RitzJob{d.R, d.R, d.ld, d.K, c.defer_ab.as<double>() + d.alpha_off,
+                             c.defer_ab.as<double>() + d.beta_off, c.defer_st.as<int32_t>() + d.steps_off, &rs[i]});
+    }
+    ritz_stage_many(c, jobs);
+    for (size_t i = 0; i < nr; ++i) {
+      rs[i].prefactor = static_cast<double>(c.defer_ritz[i].dim);
+      rs[i].particles = c.defer_ritz[i].n_up + c.defer_ritz[i].n_dn;
+      rs[i].dim = c.defer_ritz[i].dim;
+    }
   }
-  // pending spectra of the current sector become ordinary exact spectra
+  for (const DeferAcc& a : c.defer_acc) {
+    const size_t i = static_cast<size_t>(a.idx);
+    if (a.ritz) {
+      thermo_accumulate(c, rs[i]);
+    } else {
+      const DeferItem& d = c.defer_items[i];
+      thermo_accumulate_dev(c, c.defer_ev.as<double>() + eoff[i], nullptr, d.n, 1.0, d.n_up + d.n_dn);
+    }
+  }
+  // pending spectra of the current sector become ordinary ones
   for (size_t i = 0; i < nb; ++i) {
     const DeferItem& d = c.defer_items[i];
     if (d.sec_gen != c.sec_gen) continue;
@@ -409,9 +439,19 @@ void flush_exact(Ctx& c) {
     it->second.ev_off = off;
     it->second.pending = -1;
   }
+  for (size_t i = 0; i < nr; ++i) {
+    const DeferRitz& d = c.defer_ritz[i];
+    if (d.sec_gen != c.sec_gen) continue;
+    auto it = c.spec.find({d.mx, d.my});
+    if (it == c.spec.end() || it->second.pending_ritz != static_cast<int>(i)) continue;
+    it->second = rs[i];
+  }
   c.defer_items.clear();
+  c.defer_ritz.clear();
   c.defer_acc.clear();
   c.defer_asz = 0;
+  c.defer_ab_used = 0;
+  c.defer_st_used = 0;
 }
 
 }  // namespace ftlm

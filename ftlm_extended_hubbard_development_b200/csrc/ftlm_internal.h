@@ -137,7 +137,8 @@ struct Spectrum {
   double prefactor = 1.0;
   int particles = 0;
   int64_t dim = 0;
-  int pending = -1;  // exact block queued for a deferred solve: index into Ctx::defer_items
+  int pending = -1;       // exact block queued for a deferred solve: index into Ctx::defer_items
+  int pending_ritz = -1;  // small FTLM block whose Ritz stage is deferred: index into Ctx::defer_ritz
 };
 
 // An exact block whose dense matrix waits in the deferred pool.
@@ -145,6 +146,21 @@ struct DeferItem {
   int n_up, n_dn, mx, my;
   int64_t n, aoff;   // dimension, offset (complex entries) of its matrix in defer_arena
   int64_t sec_gen;   // sector generation it was assembled in
+};
+
+// A small FTLM block whose Lanczos coefficients wait in the deferred pool.
+struct DeferRitz {
+  int n_up, n_dn, mx, my;
+  int R, ld, K;
+  int64_t alpha_off, beta_off;  // doubles into defer_ab ([K][ld] each)
+  int64_t steps_off;            // int32 into defer_st ([R])
+  int64_t dim, sec_gen;
+};
+
+// A queued accumulation: an exact (ritz = false) or FTLM block of the pool.
+struct DeferAcc {
+  bool ritz;
+  int idx;
 };
 
 struct Profile {
@@ -221,14 +237,17 @@ struct Ctx {
   DBuf ritz_tmp, ritz_out, ritz_meta, scan_tmp;
   // exact batch
   DBuf dense_arena, dense_meta, dense_out;
-  // deferred exact blocks (ftlm_exact_defer): matrices of any number of
-  // sectors, diagonalised together by flush_exact; queued accumulations are
-  // indices into defer_items
-  bool exact_defer = false;
+  // deferred block spectra (ftlm_spectra_defer): dense matrices of exact
+  // blocks and Lanczos coefficients of small FTLM blocks of any number of
+  // sectors, solved together by flush_deferred, then the queued accumulations
+  bool spectra_defer = false;
   DBuf defer_arena, defer_ev, defer_work;
   int64_t defer_asz = 0;
   std::vector<DeferItem> defer_items;
-  std::vector<int> defer_acc;
+  DBuf defer_ab, defer_st;
+  int64_t defer_ab_used = 0, defer_st_used = 0;
+  std::vector<DeferRitz> defer_ritz;
+  std::vector<DeferAcc> defer_acc;
   // small-block FTLM batch: CSR arenas, task list, per-vector step counts
   DBuf sb_rp, sb_col, sb_val, sb_diag, sb_meta, sb_steps;
   // spectra of the current sector's blocks (device arena)
@@ -332,10 +351,13 @@ void run_exact_blocks(Ctx& c, const std::vector<std::pair<int, int>>& blocks);
 // first when they would push it past kDeferPoolBytes) and registers them as
 // pending spectra of the current sector.
 void queue_exact_blocks(Ctx& c, const std::vector<std::pair<int, int>>& blocks);
-// Diagonalises every pooled matrix in one launch, runs the queued
-// accumulations in queue order and turns the current sector's pending
-// spectra into ordinary ones; empties the pool.
-void flush_exact(Ctx& c);
+// Diagonalises every pooled matrix in one launch, runs the Ritz stage of
+// every pooled FTLM block in one more, then the queued accumulations in
+// queue order, and turns the current sector's pending spectra into ordinary
+// ones; empties the pool.
+void flush_deferred(Ctx& c);
+// Bytes held by the pool (matrices and Lanczos coefficients).
+int64_t defer_pool_bytes(const Ctx& c);
 constexpr int64_t kDeferPoolBytes = int64_t(4) << 30;
 // Thermo
 void thermo_configure(Ctx& c, int nbeta, const double* beta, int nmu, const double* mu);

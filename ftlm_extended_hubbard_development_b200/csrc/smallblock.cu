@@ -337,6 +337,35 @@ void run_small_ftlm_blocks(Ctx& c, const std::vector<std::pair<int, int>>& block
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
   }
+  if (c.spectra_defer) {
+    // Lanczos coefficients into the pool; the Ritz stage runs for every
+    // pooled block of every sector in one launch when the pool is flushed
+    const int64_t add = static_cast<int64_t>(sizeof(double)) * 2 * ab_tot + static_cast<int64_t>(sizeof(int32_t)) * st_tot;
+    if (defer_pool_bytes(c) > 0 && defer_pool_bytes(c) + add > kDeferPoolBytes) flush_deferred(c);
+    const int64_t ab0 = c.defer_ab_used, st0 = c.defer_st_used;
+    c.defer_ab.ensure_keep(sizeof(double) * (ab0 + 2 * ab_tot), c.stream);
+    c.defer_st.ensure_keep(sizeof(int32_t) * (st0 + st_tot), c.stream);
+    FTLM_CUDA(cudaMemcpyAsync(c.defer_ab.as<double>() + ab0, c.lz_alpha.p, sizeof(double) * ab_tot,
+                              cudaMemcpyDeviceToDevice, c.stream));
+    FTLM_CUDA(cudaMemcpyAsync(c.defer_ab.as<double>() + ab0 + ab_tot, c.lz_beta.p, sizeof(double) * ab_tot,
+                              cudaMemcpyDeviceToDevice, c.stream));
+    FTLM_CUDA(cudaMemcpyAsync(c.defer_st.as<int32_t>() + st0, c.sb_steps.p, sizeof(int32_t) * st_tot,
+                              cudaMemcpyDeviceToDevice, c.stream));
+    c.defer_ab_used = ab0 + 2 * ab_tot;
+    c.defer_st_used = st0 + st_tot;
+    for (const Item& it : items) {
+      Spectrum s;
+      s.exact = false;
+      s.prefactor = static_cast<double>(it.dim);
+      s.particles = c.sec.n_up + c.sec.n_dn;
+      s.dim = it.dim;
+      s.pending_ritz = static_cast<int>(c.defer_ritz.size());
+      c.spec[{it.mx, it.my}] = s;
+      c.defer_ritz.push_back(DeferRitz{c.sec.n_up, c.sec.n_dn, it.mx, it.my, R, ld, it.K, ab0 + it.d.ab_off,
+                                       ab0 + ab_tot + it.d.ab_off, st0 + it.d.steps_off, it.dim, c.sec_gen});
+    }
+    return;
+  }
   // Ritz values and weights per block, then compaction into the spectra arena
   std::vector<Spectrum> spec(items.size());
   std::vector<RitzJob> jobs;

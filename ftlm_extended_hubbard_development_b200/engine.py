@@ -64,7 +64,7 @@ class _Profile(C.Structure):
 EXPORTS = [
     "ftlm_abi_version", "ftlm_device_code_version", "ftlm_ctx_create", "ftlm_ctx_destroy", "ftlm_last_error",
     "ftlm_sector_prepare", "ftlm_block_spectrum", "ftlm_spectra_reset", "ftlm_blocks_exact_batched",
-    "ftlm_exact_defer", "ftlm_exact_flush", "ftlm_blocks_ftlm_batched",
+    "ftlm_spectra_defer", "ftlm_spectra_flush", "ftlm_blocks_ftlm_batched",
     "ftlm_thermo_configure", "ftlm_thermo_accumulate_block", "ftlm_thermo_accumulate_host",
     "ftlm_thermo_read", "ftlm_block_apply", "ftlm_block_lanczos",
     "ftlm_debug_sector_parents", "ftlm_debug_sector_relations", "ftlm_debug_block_csr",
@@ -96,8 +96,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "ftlm_block_spectrum": ([vp, i32, i32, i32, vp, vp, sz, P(sz), P(d)], C.c_int),
         "ftlm_spectra_reset": ([vp], C.c_int),
         "ftlm_blocks_exact_batched": ([vp, vp, vp, i32], C.c_int),
-        "ftlm_exact_defer": ([vp, i32], C.c_int),
-        "ftlm_exact_flush": ([vp], C.c_int),
+        "ftlm_spectra_defer": ([vp, i32], C.c_int),
+        "ftlm_spectra_flush": ([vp], C.c_int),
         "ftlm_blocks_ftlm_batched": ([vp, vp, vp, i32], C.c_int),
         "ftlm_thermo_configure": ([vp, i32, vp, i32, vp], C.c_int),
         "ftlm_thermo_accumulate_block": ([vp, i32, i32], C.c_int),
@@ -241,13 +241,14 @@ class Engine:
         my = np.array([b[1] for b in blocks], np.int32)
         self._check(self.lib.ftlm_blocks_exact_batched(self.h, _p(mx), _p(my), len(blocks)))
 
-    def exact_defer(self, on: bool = True):
-        """Pool the dense matrices of exact blocks across sectors and solve
-        them together (ftlm_exact_defer); off flushes the pool."""
-        self._check(self.lib.ftlm_exact_defer(self.h, int(bool(on))))
+    def spectra_defer(self, on: bool = True):
+        """Pool the exact blocks' matrices and the small FTLM blocks' Lanczos
+        coefficients across sectors and solve them together
+        (ftlm_spectra_defer); off flushes the pool."""
+        self._check(self.lib.ftlm_spectra_defer(self.h, int(bool(on))))
 
-    def exact_flush(self):
-        self._check(self.lib.ftlm_exact_flush(self.h))
+    def spectra_flush(self):
+        self._check(self.lib.ftlm_spectra_flush(self.h))
 
     def blocks_ftlm_batched(self, blocks):
         """FTLM spectra of several blocks; the small ones in one persistent launch."""
@@ -357,7 +358,7 @@ def run_curve(model: Model, betas, mu, opts: RunOpts | None = None, ed: bool = F
     eng = engine or Engine(model, opts)
     try:
         eng.thermo_configure(betas, mu)
-        eng.exact_defer(True)  # exact blocks of all sectors in one dense-solver launch
+        eng.spectra_defer(True)  # the small blocks of all sectors in one dense-solver and one Ritz launch
         n = model.sites
         for nu in range(n + 1):
             for nd in range(n + 1):
@@ -370,7 +371,7 @@ def run_curve(model: Model, betas, mu, opts: RunOpts | None = None, ed: bool = F
                 for b in blocks:
                     eng.thermo_accumulate_block(*b)
         emin, z, ns, n2 = eng.thermo_read()
-        eng.exact_defer(False)
+        eng.spectra_defer(False)
     finally:
         if own:
             eng.close()

@@ -204,7 +204,7 @@ def shard_accumulators(model: Model, betas, mu, opts: RunOpts | None = None, ed:
     eng = Engine(model, opts)
     try:
         eng.thermo_configure(betas, mu)
-        eng.exact_defer(True)  # as run_curve: one dense-solver launch for all exact blocks
+        eng.spectra_defer(True)  # as run_curve: the small blocks of all sectors solved together
         for nu in range(model.sites + 1):
             for nd in range(model.sites + 1):
                 if (nu, nd) not in mine:

@@ -137,21 +137,27 @@ int ftlm_spectra_reset(ftlm_ctx* ctx);
 int ftlm_blocks_exact_batched(ftlm_ctx* ctx, const int32_t* mx, const int32_t* my,
                               int32_t nblocks);
 
-/* Deferred exact blocks across sectors (the reference diagonalises each
- * exact block as its sector loop reaches it, main.cpp:1519-1534 with
- * 847-911). With on != 0, ftlm_blocks_exact_batched only assembles the
- * blocks' dense matrices into a device pool, and ftlm_thermo_accumulate_block
- * of such a block is queued. ftlm_exact_flush diagonalises every pooled
- * matrix, of any number of sectors, in ONE launch of the dense solver, then
- * runs the queued accumulations in the order they were queued. A sector's
- * exact blocks alone keep few SMs busy; a curve's keep all of them.
- * The pool is flushed implicitly by ftlm_thermo_read, ftlm_thermo_configure
- * (before the reset), ftlm_block_spectrum of a pooled block,
- * ftlm_exact_defer(ctx, 0), and before a batch that would take the pool
- * past 4 GiB of matrices. Accumulation order changes, so the sums differ
- * from the immediate path by rounding only. Off by default. */
-int ftlm_exact_defer(ftlm_ctx* ctx, int32_t on);
-int ftlm_exact_flush(ftlm_ctx* ctx);
+/* Deferred block spectra across sectors (the reference solves each block as
+ * its sector loop reaches it, main.cpp:1519-1534 with 847-911 and 996-1113).
+ * With on != 0, ftlm_blocks_exact_batched only assembles the exact blocks'
+ * dense matrices into a device pool, ftlm_blocks_ftlm_batched keeps the
+ * Lanczos coefficients of its small blocks (<= FTLM_SMALL_BLOCK_MAX rows)
+ * there instead of running their Ritz stage, and
+ * ftlm_thermo_accumulate_block of a pooled block is queued.
+ * ftlm_spectra_flush diagonalises every pooled matrix, of any number of
+ * sectors, in ONE launch of the dense solver and runs the Ritz stage of every
+ * pooled FTLM block in ONE more, then runs the queued accumulations in the
+ * order they were queued. A sector's blocks alone keep few SMs busy; a
+ * curve's keep all of them. The pool is flushed implicitly by
+ * ftlm_thermo_read, ftlm_thermo_configure (before the reset),
+ * ftlm_block_spectrum of a pooled block, ftlm_spectra_defer(ctx, 0), and
+ * before a batch that would take the pool past 4 GiB. Pooled spectra are
+ * bit-identical to the immediate ones; the accumulation order changes, so
+ * the sums differ from the immediate path by rounding only. A Ritz stage
+ * that fails to converge is reported by the call that flushes. Off by
+ * default; large FTLM blocks are not pooled. */
+int ftlm_spectra_defer(ftlm_ctx* ctx, int32_t on);
+int ftlm_spectra_flush(ftlm_ctx* ctx);
 
 /* FTLM spectra of several blocks of the prepared sector (run_ftlm_block,
  * main.cpp:996-1113, for a list of blocks). Blocks of at most
