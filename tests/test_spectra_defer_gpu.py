@@ -70,7 +70,7 @@ def test_pooled_curve_equals_sector_by_sector(ed):
         got, _, _ = _curve(b, True, ed)
         la, lb = a.profile()["kernel_launches"], b.profile()["kernel_launches"]
     _close(got, ref)
-    assert n_exact > 10 and (ed or n_small > 10)
+    assert n_exact > 10 and (ed or n_small > 5)  # 4x2 at threshold 256: 72 and 9 sectors
     assert la - lb == max(n_exact - 1, 0) + 2 * max(n_small - 1, 0), (la, lb, n_exact, n_small)
 
 
